@@ -1,0 +1,114 @@
+/* neighborlist_b200.h -- C ABI of the B200 neighbour-list library.
+ *
+ * Drop-in boundary for the search path of solccp/neighborlist-rs.  Each entry
+ * point names the reference interface it replaces (paths inside that
+ * project).  Conventions:
+ *   - positions: n x 3 float64, row-major (x0 y0 z0 x1 ...), host memory;
+ *   - cell: 9 float64, row-major H whose COLUMNS are the lattice vectors
+ *     (Matrix3::new argument order, src/api.rs:93-98); NULL = no cell
+ *     (auto-box: orthorhombic, origin 0, no periodicity, src/single.rs:21-58);
+ *   - pbc: 3 bytes (0/1); honoured by the brute-force minimum-image path only,
+ *     exactly like the reference (the cell-list path images every axis);
+ *   - results: exact-sized, library-owned pinned host arrays,
+ *     edge_index = [src_0..src_{M-1}, dst_0..dst_{M-1}] int64 (the layout of
+ *     NeighborList::edge_index, src/api.rs:10-17) and shift = [x0 y0 z0 x1 ...]
+ *     int32; release them with nlb_result_free.
+ * Every function returns NLB_OK or an error code; nlb_last_error() gives the
+ * calling thread's last message (the reference's Err(String) texts).
+ * All entry points are thread-safe: each host thread gets its own CUDA stream
+ * and device workspace on the current device.
+ */
+#ifndef NEIGHBORLIST_B200_H
+#define NEIGHBORLIST_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NLB_OK 0
+#define NLB_ERR_VALUE 1 /* invalid input; message from nlb_last_error() */
+#define NLB_ERR_CUDA 2  /* CUDA failure (no device, launch or copy error) */
+#define NLB_ERR_NOMEM 3 /* device or pinned-host allocation failed */
+
+typedef struct nlb_result {
+  int64_t n_edges;     /* M */
+  int64_t* edge_index; /* 2*M int64: sources then destinations */
+  int32_t* shift;      /* 3*M int32 */
+} nlb_result;
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* nlb_last_error(void);
+
+/* Single system, one cutoff.
+ * Replaces neighborlist_rs::build_neighborlists (src/api.rs:20-38) and the
+ * search behind the Python build_neighborlists (src/python_api.rs:141-186,
+ * src/single.rs:8-90).  `parallel` is accepted for signature parity and does
+ * not change the result (the reference's serial and parallel paths produce
+ * the same edges in the same order). */
+int nlb_build(const double* positions, int64_t n_atoms, double cutoff, const double* cell,
+              const uint8_t* pbc, int parallel, nlb_result* out);
+
+/* Single system, k cutoffs in one traversal (grid at the largest cutoff);
+ * outs[q] receives the list of cutoffs[q].  disjoint != 0 puts each pair in
+ * the first ascending shell only.
+ * Replaces neighborlist_rs::single::search_single_multi (src/single.rs:92-164)
+ * behind build_neighborlists_multi (src/python_api.rs:237-309). */
+int nlb_build_multi(const double* positions, int64_t n_atoms, const double* cutoffs,
+                    int32_t n_cutoffs, const double* cell, const uint8_t* pbc, int disjoint,
+                    nlb_result* outs);
+
+/* Batched systems: batch[i] is atom i's system id; a new system starts
+ * wherever the id changes (src/batch.rs:25-38).  cells: n_cells x 9 (rows of
+ * H as above) or NULL (every system auto-boxed); pbcs: n_cells x 3;
+ * has_cell: n_cells flags, 0 = None (auto-box).  Atom indices in the output
+ * are global (offset by each system's first atom).
+ * Replaces neighborlist_rs::build_neighborlists_batch (src/api.rs:43-84) and
+ * batch::search_batch (src/batch.rs:10-147). */
+int nlb_build_batch(const double* positions, int64_t n_atoms, const int32_t* batch,
+                    int64_t n_batch, double cutoff, const double* cells, const uint8_t* pbcs,
+                    const uint8_t* has_cell, int64_t n_cells, int parallel, nlb_result* out);
+
+/* Batched systems, k cutoffs.
+ * Replaces neighborlist_rs::batch::search_batch_multi (src/batch.rs:149-290). */
+int nlb_build_batch_multi(const double* positions, int64_t n_atoms, const int32_t* batch,
+                          int64_t n_batch, const double* cutoffs, int32_t n_cutoffs,
+                          const double* cells, const uint8_t* pbcs, const uint8_t* has_cell,
+                          int64_t n_cells, int disjoint, nlb_result* outs);
+
+/* Releases both arrays of a result (safe on a zeroed struct). */
+void nlb_result_free(nlb_result* r);
+/* Releases one array obtained from a result (for callers that hand the two
+ * arrays to separate owners, e.g. two numpy arrays). */
+void nlb_host_free(void* p);
+
+/* Dispatch thresholds (src/config.rs:4-40).  The brute-force threshold decides
+ * brute force vs cell list and therefore the output order; the parallel
+ * threshold selects the reference's serial/parallel CPU variant and has no
+ * effect on the result; the stack threshold is kept for API parity and is
+ * clamped to 1024 like the reference. */
+size_t nlb_get_brute_force_threshold(void);
+void nlb_set_brute_force_threshold(size_t v);
+size_t nlb_get_parallel_threshold(void);
+void nlb_set_parallel_threshold(size_t v);
+size_t nlb_get_stack_threshold(void);
+void nlb_set_stack_threshold(size_t v);
+
+/* Cell helpers behind the Python PyCell class (src/python_api.rs:15-99).
+ * nlb_cell_check: 0 if H is invertible, NLB_ERR_VALUE ("Cell matrix is not
+ * invertible", src/cell.rs:18-21) otherwise.
+ * nlb_cell_wrap: Cell::wrap (src/cell.rs:52-72): fractional wrap on the
+ * periodic axes only. */
+int nlb_cell_check(const double* cell);
+int nlb_cell_wrap(const double* cell, const uint8_t* pbc, const double* position, double* out);
+
+/* Library version string. */
+const char* nlb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEIGHBORLIST_B200_H */

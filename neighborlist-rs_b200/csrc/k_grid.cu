@@ -1,0 +1,230 @@
+// k_grid.cu -- cell-list build on the device (src/search.rs:92-264).
+//
+// Order produced (identical to the reference): atoms grouped by bin in bin
+// Morton-rank order; inside a bin by atom Morton key (ties: original index).
+//
+//   k_rank_table : Morton rank of every bin, counted analytically (no sort):
+//                  rank(c) = #grid points whose 63-bit Morton code is < code(c).
+//   k_prep       : per atom: fraction, wrap, Morton key, bin rank, bin histogram.
+//   (scan)       : bin histogram -> bin starts.
+//   k_scatter    : atoms -> bin segments (arbitrary order inside a segment).
+//   k_binsort    : one CTA per bin sorts its (key, index) pairs -- bitonic in
+//                  shared memory up to kSortCap, merge path through global
+//                  scratch above it -- and gathers the sorted SoA arrays
+//                  (wrapped positions, wrap shifts, original indices).
+#include "nlb_kernels.h"
+
+namespace nlb {
+
+namespace {
+
+constexpr int kSortThreads = 128;
+constexpr int kSortCap = 2048;  // elements sorted entirely in shared memory
+
+// Grid points p (0 <= p_a < nb_a) whose Morton code is smaller than that of c.
+__device__ int64_t morton_rank(const int32_t c[3], const int32_t nb[3]) {
+  int64_t rank = 0;
+  for (int l = 20; l >= 0; --l) {
+    for (int a = 2; a >= 0; --a) {  // code bit 3l+a, most significant first
+      if (!((c[a] >> l) & 1)) continue;
+      int64_t cnt = 1;
+      for (int b = 0; b < 3; ++b) {
+        int64_t lo, len;
+        if (b == a) {
+          lo = ((int64_t)(c[b] >> (l + 1))) << (l + 1);
+          len = (int64_t)1 << l;
+        } else if (b < a) {
+          lo = ((int64_t)(c[b] >> (l + 1))) << (l + 1);
+          len = (int64_t)1 << (l + 1);
+        } else {
+          lo = ((int64_t)(c[b] >> l)) << l;
+          len = (int64_t)1 << l;
+        }
+        int64_t hi = lo + len;
+        if (hi > nb[b]) hi = nb[b];
+        const int64_t w = hi - lo;
+        if (w <= 0) {
+          cnt = 0;
+          break;
+        }
+        cnt *= w;
+      }
+      rank += cnt;
+    }
+  }
+  return rank;
+}
+
+__global__ void k_rank_table(GridParams g, int32_t* __restrict__ rank_of_bin) {
+  const int64_t lin = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (lin >= g.total_bins) return;
+  int32_t c[3];
+  c[0] = (int32_t)(lin % g.nb[0]);
+  c[1] = (int32_t)((lin / g.nb[0]) % g.nb[1]);
+  c[2] = (int32_t)(lin / ((int64_t)g.nb[0] * g.nb[1]));
+  rank_of_bin[lin] = (int32_t)morton_rank(c, g.nb);
+}
+
+__global__ void k_prep(GridParams g, const double* __restrict__ pos, int64_t n,
+                       const int32_t* __restrict__ rank_of_bin, uint64_t* __restrict__ key,
+                       int32_t* __restrict__ rank, int32_t* __restrict__ bin_count) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const AtomWrap w = wrap_atom(g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  const int64_t lin = w.bin[0] + (int64_t)g.nb[0] * (w.bin[1] + (int64_t)g.nb[1] * w.bin[2]);
+  const int32_t r = rank_of_bin[lin];
+  key[i] = w.key;
+  rank[i] = r;
+  atomicAdd(&bin_count[r], 1);
+}
+
+__global__ void k_scatter(const uint64_t* __restrict__ key, const int32_t* __restrict__ rank,
+                          int64_t n, const int64_t* __restrict__ bin_start,
+                          int32_t* __restrict__ bin_fill, uint64_t* __restrict__ skey,
+                          int32_t* __restrict__ sidx) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t r = rank[i];
+  const int64_t slot = bin_start[r] + atomicAdd(&bin_fill[r], 1);
+  skey[slot] = key[i];
+  sidx[slot] = (int32_t)i;
+}
+
+__device__ __forceinline__ bool pair_less(uint64_t ka, int32_t ia, uint64_t kb, int32_t ib) {
+  return ka < kb || (ka == kb && ia < ib);
+}
+
+// Bitonic sort of cnt (<= kSortCap) pairs held in shared memory.
+__device__ void smem_bitonic(uint64_t* k, int32_t* v, int cnt) {
+  int p = 1;
+  while (p < cnt) p <<= 1;
+  for (int i = cnt + threadIdx.x; i < p; i += blockDim.x) {
+    k[i] = ~0ull;
+    v[i] = 0x7fffffff;
+  }
+  __syncthreads();
+  for (int size = 2; size <= p; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < p; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const bool gt = pair_less(k[j], v[j], k[i], v[i]);
+          if (gt == up) {
+            const uint64_t tk = k[i];
+            k[i] = k[j];
+            k[j] = tk;
+            const int32_t tv = v[i];
+            v[i] = v[j];
+            v[j] = tv;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+    k_binsort(GridParams g, const double* __restrict__ pos, const int64_t* __restrict__ bin_start,
+              uint64_t* __restrict__ skey, int32_t* __restrict__ sidx,
+              uint64_t* __restrict__ skey2, int32_t* __restrict__ sidx2,
+              double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz,
+              SlotMeta* __restrict__ meta) {
+  __shared__ uint64_t sk[kSortCap];
+  __shared__ int32_t sv[kSortCap];
+  const int64_t r = blockIdx.x;
+  const int64_t s = bin_start[r];
+  const int64_t e = bin_start[r + 1];
+  const int64_t cnt = e - s;
+  if (cnt == 0) return;
+
+  const int32_t* final_idx = sidx;
+  // Sort chunks of kSortCap in shared memory (the whole bin when it fits).
+  for (int64_t c0 = 0; c0 < cnt; c0 += kSortCap) {
+    const int m = (int)(cnt - c0 < kSortCap ? cnt - c0 : kSortCap);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      sk[i] = skey[s + c0 + i];
+      sv[i] = sidx[s + c0 + i];
+    }
+    __syncthreads();
+    smem_bitonic(sk, sv, m);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      skey[s + c0 + i] = sk[i];
+      sidx[s + c0 + i] = sv[i];
+    }
+    __syncthreads();
+  }
+  if (cnt > kSortCap) {
+    // Merge sorted runs pairwise (merge path per output element), ping-ponging
+    // between the bin's range of (skey, sidx) and (skey2, sidx2).
+    uint64_t* ak = skey + s;
+    int32_t* av = sidx + s;
+    uint64_t* bk = skey2 + s;
+    int32_t* bv = sidx2 + s;
+    for (int64_t w = kSortCap; w < cnt; w <<= 1) {
+      for (int64_t d = threadIdx.x; d < cnt; d += blockDim.x) {
+        const int64_t a0 = (d / (2 * w)) * (2 * w);
+        const int64_t la = cnt - a0 < w ? cnt - a0 : w;
+        const int64_t lb = cnt - a0 - la < w ? cnt - a0 - la : w;
+        const int64_t dd = d - a0;
+        const uint64_t* A = ak + a0;
+        const int32_t* Av = av + a0;
+        const uint64_t* B = ak + a0 + la;
+        const int32_t* Bv = av + a0 + la;
+        int64_t lo = dd > lb ? dd - lb : 0, hi = dd < la ? dd : la;
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) >> 1;
+          if (pair_less(A[mid], Av[mid], B[dd - mid - 1], Bv[dd - mid - 1]))
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        const int64_t ia = lo, ib = dd - lo;
+        const bool take_a = ib >= lb || (ia < la && pair_less(A[ia], Av[ia], B[ib], Bv[ib]));
+        bk[d] = take_a ? A[ia] : B[ib];
+        bv[d] = take_a ? Av[ia] : Bv[ib];
+      }
+      __syncthreads();
+      uint64_t* tk = ak;
+      ak = bk;
+      bk = tk;
+      int32_t* tv = av;
+      av = bv;
+      bv = tv;
+    }
+    final_idx = av - s;
+  }
+  // Gather the sorted slots: wrapped positions, wrap shifts, original index.
+  for (int64_t p = s + threadIdx.x; p < e; p += blockDim.x) {
+    const int32_t idx = final_idx[p];
+    const AtomWrap w = wrap_atom(g, pos[3 * (int64_t)idx], pos[3 * (int64_t)idx + 1],
+                                 pos[3 * (int64_t)idx + 2]);
+    px[p] = w.wx;
+    py[p] = w.wy;
+    pz[p] = w.wz;
+    SlotMeta mt;
+    mt.sx = w.s[0];
+    mt.sy = w.s[1];
+    mt.sz = w.s[2];
+    mt.orig = idx;
+    meta[p] = mt;
+  }
+}
+
+}  // namespace
+
+void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const GridBuffers& b,
+                       cudaStream_t s) {
+  const int T = 256;
+  k_rank_table<<<(unsigned)((g.total_bins + T - 1) / T), T, 0, s>>>(g, b.rank_of_bin);
+  k_prep<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(g, pos, n, b.rank_of_bin, b.key, b.rank,
+                                                    b.bin_count);
+  exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
+  k_scatter<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(b.key, b.rank, n, b.bin_start, b.bin_fill,
+                                                       b.skey, b.sidx);
+  k_binsort<<<(unsigned)g.total_bins, kSortThreads, 0, s>>>(
+      g, pos, b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta);
+}
+
+}  // namespace nlb

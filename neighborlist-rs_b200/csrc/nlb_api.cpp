@@ -1,0 +1,520 @@
+// nlb_api.cpp -- C ABI, dispatch and device workspace management.
+//
+// Host-side counterpart of the reference's drivers (src/single.rs,
+// src/batch.rs, src/api.rs): validation, cell construction, the brute-force
+// / cell-list dispatch, and the count -> scan -> emit orchestration of the
+// CUDA kernels on a per-thread stream.  Results come back in pinned host
+// memory from a reuse pool, so the device-to-host copy of the edge arrays
+// runs at full PCIe rate.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/neighborlist_b200.h"
+#include "nlb_geometry.h"
+#include "nlb_internal.h"
+#include "nlb_kernels.h"
+
+namespace nlb {
+
+// ------------------------------------------------------------------ errors
+
+thread_local std::string g_last_error;
+
+Status fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return Status{code};
+}
+
+Status cuda_fail(cudaError_t e, const char* what) {
+  return fail(NLB_ERR_CUDA, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------ config
+
+std::atomic<uint64_t> g_bf_threshold{1000};   // src/config.rs DEFAULT_BRUTE_FORCE_THRESHOLD
+std::atomic<uint64_t> g_par_threshold{300};   // DEFAULT_PARALLEL_THRESHOLD
+std::atomic<uint64_t> g_stack_threshold{1000};  // DEFAULT_STACK_THRESHOLD
+
+// ------------------------------------------------------------------ pinned pool
+
+namespace {
+
+struct PinnedPool {
+  std::mutex mu;
+  std::multimap<size_t, void*> free_blocks;  // size -> block
+  std::unordered_map<void*, size_t> sizes;   // every block handed out or cached
+  size_t cached = 0;
+  static constexpr size_t kMaxCached = size_t(8) << 30;
+
+  void* alloc(size_t bytes) {
+    bytes = std::max<size_t>(bytes, 256);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = free_blocks.lower_bound(bytes);
+      if (it != free_blocks.end() && it->first <= 2 * bytes + (size_t(1) << 20)) {
+        void* p = it->second;
+        cached -= it->first;
+        free_blocks.erase(it);
+        return p;
+      }
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    sizes[p] = bytes;
+    return p;
+  }
+
+  void release(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = sizes.find(p);
+    if (it == sizes.end()) return;  // not ours
+    const size_t sz = it->second;
+    while (cached + sz > kMaxCached && !free_blocks.empty()) {
+      auto big = std::prev(free_blocks.end());
+      cached -= big->first;
+      sizes.erase(big->second);
+      cudaFreeHost(big->second);
+      free_blocks.erase(big);
+    }
+    free_blocks.emplace(sz, p);
+    cached += sz;
+  }
+};
+
+PinnedPool& pinned_pool() {
+  static PinnedPool* pool = new PinnedPool();  // never destroyed (process lifetime)
+  return *pool;
+}
+
+}  // namespace
+
+void* pinned_alloc(size_t bytes) { return pinned_pool().alloc(bytes); }
+void pinned_release(void* p) { pinned_pool().release(p); }
+
+// ------------------------------------------------------------------ context
+
+void* Ctx::raw(int slot, size_t bytes) {
+  Buf& b = bufs[slot];
+  if (bytes > b.cap) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    size_t cap = std::max<size_t>(bytes + bytes / 4, 4096);
+    if (cudaMalloc(&b.p, cap) != cudaSuccess) {
+      cudaGetLastError();
+      b.p = nullptr;
+      return nullptr;
+    }
+    b.cap = cap;
+  }
+  return b.p;
+}
+
+Status get_ctx(Ctx** out) {
+  thread_local std::unordered_map<int, Ctx*> ctxs;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice (is a CUDA device present?)");
+  auto it = ctxs.find(dev);
+  if (it != ctxs.end()) {
+    *out = it->second;
+    return Status{NLB_OK};
+  }
+  Ctx* c = new Ctx();  // lives for the thread's lifetime; never freed at exit
+  c->device = dev;
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+  e = cudaHostAlloc((void**)&c->h_small, sizeof(int64_t) * kSmallHost, cudaHostAllocDefault);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+  ctxs[dev] = c;
+  *out = c;
+  return Status{NLB_OK};
+}
+
+void ensure_smem_attr(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> done;  // (func, device) -> bytes
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto key = std::make_pair(func, dev);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= bytes) return;
+  cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  done[key] = bytes;
+}
+
+// ------------------------------------------------------------------ one system
+
+// Counts one system's edges per sorted cutoff.  Leaves the per-atom offsets
+// in the context for emit_system().  Synchronizes once (to read the totals).
+Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
+  const int64_t n = sp.n;
+  const int32_t k = (int32_t)sp.rc_sq.size();
+  cudaStream_t s = c.stream;
+  sp.counts = slot<uint32_t>(c, kSlotCounts, (size_t)k * (n + 1));
+  sp.offs = slot<int64_t>(c, kSlotOffs, (size_t)k * (n + 1) + 1);
+  int64_t* scan_tmp =
+      slot<int64_t>(c, kSlotScanTmp, (size_t)scan_tmp_elems(std::max<int64_t>(
+                                          (int64_t)k * (n + 1), sp.grid.total_bins)));
+  if (!sp.counts || !sp.offs || !scan_tmp) return fail(NLB_ERR_NOMEM, "device allocation failed");
+
+  if (sp.method == Method::kCellList) {
+    GridBuffers& b = sp.gb;
+    const int64_t nb = sp.grid.total_bins;
+    b.rank_of_bin = slot<int32_t>(c, kSlotRankTab, nb);
+    b.bin_count = slot<int32_t>(c, kSlotBinCount, nb);
+    b.bin_fill = slot<int32_t>(c, kSlotBinFill, nb);
+    b.bin_start = slot<int64_t>(c, kSlotBinStart, nb + 1);
+    b.key = slot<uint64_t>(c, kSlotKey, n);
+    b.rank = slot<int32_t>(c, kSlotRank, n);
+    b.skey = slot<uint64_t>(c, kSlotSkey, n);
+    b.sidx = slot<int32_t>(c, kSlotSidx, n);
+    b.skey2 = slot<uint64_t>(c, kSlotSkey2, n);
+    b.sidx2 = slot<int32_t>(c, kSlotSidx2, n);
+    b.px = slot<double>(c, kSlotPx, n);
+    b.py = slot<double>(c, kSlotPy, n);
+    b.pz = slot<double>(c, kSlotPz, n);
+    b.meta = slot<SlotMeta>(c, kSlotMeta, n);
+    b.scan_tmp = scan_tmp;
+    if (!b.rank_of_bin || !b.bin_count || !b.bin_fill || !b.bin_start || !b.key || !b.rank ||
+        !b.skey || !b.sidx || !b.skey2 || !b.sidx2 || !b.px || !b.py || !b.pz || !b.meta)
+      return fail(NLB_ERR_NOMEM, "device allocation failed");
+    cudaMemsetAsync(b.bin_count, 0, sizeof(int32_t) * nb, s);
+    cudaMemsetAsync(b.bin_fill, 0, sizeof(int32_t) * nb, s);
+    launch_grid_build(sp.grid, d_pos, n, b, s);
+  }
+  for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
+    CutoffSet cs = sp.pass(g0);
+    uint32_t* rows = sp.counts + (size_t)g0 * (n + 1);
+    if (sp.method == Method::kCellList)
+      launch_grid_count(sp.grid, sp.gb, n, cs, rows, s);
+    else
+      launch_brute_count(sp.brute, d_pos, n, cs, rows, s);
+  }
+  exclusive_scan_u32(sp.counts, (int64_t)k * (n + 1), sp.offs, scan_tmp, s);
+  // Row starts offs[q * (n + 1)], q = 0..k, in one strided copy.
+  if (k + 1 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
+  cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), sp.offs, sizeof(int64_t) * (n + 1),
+                                    sizeof(int64_t), (size_t)k + 1, cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy2DAsync");
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "count pass");
+  sp.m.resize(k);
+  for (int32_t q = 0; q < k; ++q) sp.m[q] = c.h_small[q + 1] - c.h_small[q];
+  return Status{NLB_OK};
+}
+
+// Emits one system's edges into the given device lists (per sorted cutoff).
+Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& L,
+                   const int64_t* base, int64_t index_offset) {
+  const int32_t k = (int32_t)sp.rc_sq.size();
+  for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
+    CutoffSet cs = sp.pass(g0);
+    EmitTargets t;
+    std::memset(&t, 0, sizeof(t));
+    for (int32_t q = 0; q < cs.k; ++q) {
+      t.src[q] = L.src[g0 + q];
+      t.dst[q] = L.dst[g0 + q];
+      t.sh[q] = L.sh[g0 + q];
+      t.base[q] = base[g0 + q];
+    }
+    t.index_offset = index_offset;
+    const int64_t* offs = sp.offs + (size_t)g0 * (sp.n + 1);
+    if (sp.method == Method::kCellList)
+      launch_grid_emit(sp.grid, sp.gb, sp.n, cs, offs, t, c.stream);
+    else
+      launch_brute_emit(sp.brute, d_pos, sp.n, cs, offs, t, c.stream);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "emit launch");
+  return Status{NLB_OK};
+}
+
+CutoffSet SystemPlan::pass(int32_t g0) const {
+  CutoffSet cs;
+  std::memset(&cs, 0, sizeof(cs));
+  const int32_t k = (int32_t)rc_sq.size();
+  cs.k = std::min<int32_t>(kMaxCutoffsPerPass, k - g0);
+  for (int32_t q = 0; q < cs.k; ++q) cs.rc_sq[q] = rc_sq[g0 + q];
+  cs.disjoint = disjoint ? 1 : 0;
+  cs.lower_sq = g0 > 0 ? rc_sq[g0 - 1] : -1.0;
+  cs.max_sq = rc_sq.back();
+  return cs;
+}
+
+// Validates and plans one system (cell or auto-box, dispatch, grid).
+Status plan_system(const double* pos_host, int64_t n, const double* cell9, const bool pbc[3],
+                   const std::vector<double>& cutoffs, bool disjoint, bool multi,
+                   SystemPlan& sp) {
+  sp.n = n;
+  sp.disjoint = disjoint;
+  const int32_t k = (int32_t)cutoffs.size();
+  double rc_max = NAN;
+  for (double r : cutoffs) rc_max = fmax_nan_ignoring(rc_max, r);
+  std::string err;
+  if (cell9) {
+    if (!make_cell(cell9, pbc, sp.cell, err)) return fail(NLB_ERR_VALUE, err);
+  } else {
+    if (!auto_box(pos_host, n, rc_max, sp.cell, err)) return fail(NLB_ERR_VALUE, err);
+  }
+  sp.order = cutoff_order(cutoffs.data(), k);
+  sp.rc_sq.resize(k);
+  for (int32_t q = 0; q < k; ++q) sp.rc_sq[q] = cutoffs[sp.order[q]] * cutoffs[sp.order[q]];
+  sp.method = choose_method(sp.cell, n, rc_max, g_bf_threshold.load(), multi);
+  if (sp.method == Method::kCellList) {
+    plan_grid(sp.cell, rc_max, sp.grid);
+    for (int a = 0; a < 3; ++a)
+      if (sp.grid.nb[a] >= (1 << 21))
+        return fail(NLB_ERR_VALUE, "cell list needs more than 2^21 bins along one axis");
+    if (sp.grid.total_bins > ((int64_t)1 << 31) - 2)
+      return fail(NLB_ERR_VALUE, "cell list needs more than 2^31 bins");
+    for (int a = 0; a < 3; ++a)
+      if (sp.grid.ns[a] < 0 || sp.grid.ns[a] > (1 << 20))
+        return fail(NLB_ERR_VALUE, "stencil too large for this cutoff and cell");
+  } else {
+    std::memcpy(sp.brute.h, sp.cell.h, sizeof(sp.brute.h));
+    std::memcpy(sp.brute.hinv, sp.cell.hinv, sizeof(sp.brute.hinv));
+    for (int a = 0; a < 3; ++a) sp.brute.pbc[a] = sp.cell.pbc[a] ? 1 : 0;
+    sp.brute.mode = sp.method == Method::kBruteIsolated ? kBruteRaw : kBruteMicMode;
+  }
+  if (n > (int64_t)INT32_MAX - 1) return fail(NLB_ERR_VALUE, "more than 2^31 atoms in one system");
+  return Status{NLB_OK};
+}
+
+// ------------------------------------------------------------------ results
+
+Status alloc_result(int64_t m, nlb_result* r) {
+  r->n_edges = m;
+  r->edge_index = static_cast<int64_t*>(pinned_alloc(sizeof(int64_t) * 2 * (size_t)m));
+  r->shift = static_cast<int32_t*>(pinned_alloc(sizeof(int32_t) * 3 * (size_t)m));
+  if (!r->edge_index || !r->shift) {
+    pinned_release(r->edge_index);
+    pinned_release(r->shift);
+    r->edge_index = nullptr;
+    r->shift = nullptr;
+    return fail(NLB_ERR_NOMEM, "pinned host allocation failed");
+  }
+  return Status{NLB_OK};
+}
+
+void zero_results(nlb_result* outs, int32_t k) {
+  for (int32_t q = 0; q < k; ++q) {
+    outs[q].n_edges = 0;
+    outs[q].edge_index = nullptr;
+    outs[q].shift = nullptr;
+  }
+}
+
+Status empty_results(nlb_result* outs, int32_t k) {
+  for (int32_t q = 0; q < k; ++q) {
+    Status st = alloc_result(0, &outs[q]);
+    if (!st.ok()) return st;
+  }
+  return Status{NLB_OK};
+}
+
+// Device output workspace for k lists of sizes m[q], laid out exactly like
+// the host results ([src | dst] per list) so each list downloads in one copy.
+Status device_outputs(Ctx& c, const std::vector<int64_t>& m, DevLists& L) {
+  int64_t tot = 0;
+  for (int64_t x : m) tot += x;
+  int64_t* ei_all = slot<int64_t>(c, kSlotOutEi, 2 * (size_t)tot);
+  int32_t* sh_all = slot<int32_t>(c, kSlotOutSh, 3 * (size_t)tot);
+  if (!ei_all || !sh_all) return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
+  L.src.resize(m.size());
+  L.dst.resize(m.size());
+  L.sh.resize(m.size());
+  int64_t acc = 0;
+  for (size_t q = 0; q < m.size(); ++q) {
+    L.src[q] = ei_all + 2 * acc;
+    L.dst[q] = ei_all + 2 * acc + m[q];
+    L.sh[q] = sh_all + 3 * acc;
+    acc += m[q];
+  }
+  return Status{NLB_OK};
+}
+
+// Copies contiguous device lists (sorted cutoff order) to pinned results in
+// input cutoff order.
+Status download_results(Ctx& c, const std::vector<int64_t>& m, const DevLists& L,
+                        const std::vector<int32_t>& order, nlb_result* outs) {
+  const int32_t k = (int32_t)m.size();
+  for (int32_t q = 0; q < k; ++q) {
+    nlb_result& r = outs[order[q]];
+    Status st = alloc_result(m[q], &r);
+    if (!st.ok()) return st;
+    if (m[q] == 0) continue;
+    cudaError_t e = cudaMemcpyAsync(r.edge_index, L.src[q], sizeof(int64_t) * 2 * m[q],
+                                    cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(r.shift, L.sh[q], sizeof(int32_t) * 3 * m[q], cudaMemcpyDeviceToHost,
+                          c.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync (results)");
+  }
+  cudaError_t e = cudaStreamSynchronize(c.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "emit pass");
+  return Status{NLB_OK};
+}
+
+Status upload_positions(Ctx& c, const double* pos, int64_t n, double** d_pos) {
+  *d_pos = slot<double>(c, kSlotPos, 3 * (size_t)n);
+  if (!*d_pos) return fail(NLB_ERR_NOMEM, "device allocation failed");
+  cudaError_t e = cudaMemcpyAsync(*d_pos, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                                  c.stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync (positions)");
+  return Status{NLB_OK};
+}
+
+bool cutoffs_valid(const double* cs, int32_t k) {
+  for (int32_t q = 0; q < k; ++q)
+    if (!std::isfinite(cs[q]) || cs[q] <= 0.0) return false;
+  return true;
+}
+
+// One system, k cutoffs, host in / host out.
+Status run_single(const double* pos, int64_t n, const double* cell9, const uint8_t* pbc,
+                  const double* cutoffs, int32_t k, bool disjoint, bool multi, nlb_result* outs) {
+  zero_results(outs, k);
+  if (k <= 0) return Status{NLB_OK};
+  if (!cutoffs_valid(cutoffs, k))
+    return fail(NLB_ERR_VALUE, multi ? "All cutoffs must be positive and finite"
+                                     : "Cutoff must be positive and finite");
+  if (n < 0) return fail(NLB_ERR_VALUE, "Positions must be (N, 3)");
+  if (n == 0) return empty_results(outs, k);
+  if (!pos) return fail(NLB_ERR_VALUE, "positions is NULL");
+  const bool pb[3] = {pbc ? pbc[0] != 0 : true, pbc ? pbc[1] != 0 : true,
+                      pbc ? pbc[2] != 0 : true};
+  SystemPlan sp;
+  std::vector<double> cs(cutoffs, cutoffs + k);
+  Status st = plan_system(pos, n, cell9, pb, cs, disjoint, multi, sp);
+  if (!st.ok()) return st;
+  Ctx* c = nullptr;
+  st = get_ctx(&c);
+  if (!st.ok()) return st;
+  double* d_pos = nullptr;
+  st = upload_positions(*c, pos, n, &d_pos);
+  if (!st.ok()) return st;
+  st = count_system(*c, sp, d_pos);
+  if (!st.ok()) return st;
+  DevLists L;
+  st = device_outputs(*c, sp.m, L);
+  if (!st.ok()) return st;
+  std::vector<int64_t> zeros(k, 0);
+  st = emit_system(*c, sp, d_pos, L, zeros.data(), 0);
+  if (!st.ok()) return st;
+  st = download_results(*c, sp.m, L, sp.order, outs);
+  if (!st.ok()) {
+    for (int32_t q = 0; q < k; ++q) nlb_result_free(&outs[q]);
+  }
+  return st;
+}
+
+}  // namespace nlb
+
+// ------------------------------------------------------------------ C ABI
+
+using namespace nlb;
+
+extern "C" {
+
+const char* nlb_last_error(void) { return g_last_error.c_str(); }
+
+const char* nlb_version(void) { return "neighborlist-b200 0.1.0 (sm_100a)"; }
+
+int nlb_build(const double* positions, int64_t n_atoms, double cutoff, const double* cell,
+              const uint8_t* pbc, int /*parallel*/, nlb_result* out) {
+  if (!out) return fail(NLB_ERR_VALUE, "out is NULL").code;
+  return run_single(positions, n_atoms, cell, pbc, &cutoff, 1, false, false, out).code;
+}
+
+int nlb_build_multi(const double* positions, int64_t n_atoms, const double* cutoffs,
+                    int32_t n_cutoffs, const double* cell, const uint8_t* pbc, int disjoint,
+                    nlb_result* outs) {
+  if (n_cutoffs > 0 && (!outs || !cutoffs)) return fail(NLB_ERR_VALUE, "outs is NULL").code;
+  return run_single(positions, n_atoms, cell, pbc, cutoffs, n_cutoffs, disjoint != 0, true, outs)
+      .code;
+}
+
+int nlb_build_batch(const double* positions, int64_t n_atoms, const int32_t* batch,
+                    int64_t n_batch, double cutoff, const double* cells, const uint8_t* pbcs,
+                    const uint8_t* has_cell, int64_t n_cells, int /*parallel*/, nlb_result* out) {
+  if (!out) return fail(NLB_ERR_VALUE, "out is NULL").code;
+  return run_batch(positions, n_atoms, batch, n_batch, &cutoff, 1, cells, pbcs, has_cell, n_cells,
+                   false, false, out)
+      .code;
+}
+
+int nlb_build_batch_multi(const double* positions, int64_t n_atoms, const int32_t* batch,
+                          int64_t n_batch, const double* cutoffs, int32_t n_cutoffs,
+                          const double* cells, const uint8_t* pbcs, const uint8_t* has_cell,
+                          int64_t n_cells, int disjoint, nlb_result* outs) {
+  if (n_cutoffs > 0 && (!outs || !cutoffs)) return fail(NLB_ERR_VALUE, "outs is NULL").code;
+  return run_batch(positions, n_atoms, batch, n_batch, cutoffs, n_cutoffs, cells, pbcs, has_cell,
+                   n_cells, disjoint != 0, true, outs)
+      .code;
+}
+
+void nlb_result_free(nlb_result* r) {
+  if (!r) return;
+  pinned_release(r->edge_index);
+  pinned_release(r->shift);
+  r->edge_index = nullptr;
+  r->shift = nullptr;
+  r->n_edges = 0;
+}
+
+void nlb_host_free(void* p) { pinned_release(p); }
+
+int nlb_cell_check(const double* cell) {
+  if (!cell) return fail(NLB_ERR_VALUE, "cell is NULL").code;
+  HostCell c;
+  std::string err;
+  const bool pb[3] = {true, true, true};
+  if (!make_cell(cell, pb, c, err)) return fail(NLB_ERR_VALUE, err).code;
+  return NLB_OK;
+}
+
+int nlb_cell_wrap(const double* cell, const uint8_t* pbc, const double* p, double* out) {
+  if (!cell || !p || !out) return fail(NLB_ERR_VALUE, "NULL argument").code;
+  HostCell c;
+  std::string err;
+  const bool pb[3] = {pbc ? pbc[0] != 0 : true, pbc ? pbc[1] != 0 : true,
+                      pbc ? pbc[2] != 0 : true};
+  if (!make_cell(cell, pb, c, err)) return fail(NLB_ERR_VALUE, err).code;
+  double f[3];
+  for (int r = 0; r < 3; ++r) {
+    const double t = c.hinv[3 * r] * p[0] + c.hinv[3 * r + 1] * p[1];
+    f[r] = t + c.hinv[3 * r + 2] * p[2];
+  }
+  for (int a = 0; a < 3; ++a)
+    if (pb[a]) f[a] = f[a] - std::floor(f[a]);
+  for (int r = 0; r < 3; ++r) {
+    const double t = c.h[3 * r] * f[0] + c.h[3 * r + 1] * f[1];
+    out[r] = t + c.h[3 * r + 2] * f[2];
+  }
+  return NLB_OK;
+}
+
+size_t nlb_get_brute_force_threshold(void) { return (size_t)g_bf_threshold.load(); }
+void nlb_set_brute_force_threshold(size_t v) { g_bf_threshold.store(v); }
+size_t nlb_get_parallel_threshold(void) { return (size_t)g_par_threshold.load(); }
+void nlb_set_parallel_threshold(size_t v) { g_par_threshold.store(v); }
+size_t nlb_get_stack_threshold(void) { return (size_t)g_stack_threshold.load(); }
+void nlb_set_stack_threshold(size_t v) { g_stack_threshold.store(std::min<size_t>(v, 1024)); }
+
+}  // extern "C"

@@ -1,0 +1,120 @@
+// nlb_internal.h -- host-side internals shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/neighborlist_b200.h"
+#include "nlb_geometry.h"
+#include "nlb_kernels.h"
+
+namespace nlb {
+
+struct Status {
+  int code;
+  bool ok() const { return code == NLB_OK; }
+};
+
+Status fail(int code, const std::string& msg);
+Status cuda_fail(cudaError_t e, const char* what);
+
+extern thread_local std::string g_last_error;
+
+// Device workspace slots (grow-only buffers, one set per host thread and device).
+enum Slot : int {
+  kSlotPos = 0,
+  kSlotRankTab,
+  kSlotBinCount,
+  kSlotBinFill,
+  kSlotBinStart,
+  kSlotKey,
+  kSlotRank,
+  kSlotSkey,
+  kSlotSidx,
+  kSlotSkey2,
+  kSlotSidx2,
+  kSlotPx,
+  kSlotPy,
+  kSlotPz,
+  kSlotMeta,
+  kSlotScanTmp,
+  kSlotCounts,
+  kSlotOffs,
+  kSlotOutEi,
+  kSlotOutSh,
+  kSlotBatch0,  // first slot owned by the batched path
+  kSlotCount = kSlotBatch0 + 32,
+};
+
+constexpr int kSmallHost = 4096;  // int64 slots of the per-context pinned scratch
+
+struct Ctx {
+  struct Buf {
+    void* p = nullptr;
+    size_t cap = 0;
+  };
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t* h_small = nullptr;  // pinned scratch for small device->host reads
+  Buf bufs[kSlotCount];
+  // Returns a device buffer of at least `bytes` for `slot` (contents are not
+  // preserved on growth), or nullptr if the allocation failed.
+  void* raw(int slot, size_t bytes);
+};
+
+Status get_ctx(Ctx** out);
+
+template <class T>
+inline T* slot(Ctx& c, int s, size_t count) {
+  return static_cast<T*>(c.raw(s, sizeof(T) * (count > 0 ? count : 1)));
+}
+
+void* pinned_alloc(size_t bytes);
+void pinned_release(void* p);
+
+// One system after planning: cell, dispatch decision, grid or brute-force
+// parameters, cutoffs in ascending order, and (after count_system) the
+// per-cutoff edge totals and per-atom offsets on the device.
+struct SystemPlan {
+  int64_t n = 0;
+  HostCell cell;
+  Method method = Method::kCellList;
+  GridParams grid{};
+  BruteParams brute{};
+  GridBuffers gb{};
+  bool disjoint = false;
+  std::vector<int32_t> order;   // sorted position q -> input cutoff index
+  std::vector<double> rc_sq;    // ascending squared cutoffs
+  std::vector<int64_t> m;       // edges per sorted cutoff (after count)
+  uint32_t* counts = nullptr;
+  int64_t* offs = nullptr;
+  CutoffSet pass(int32_t g0) const;
+};
+
+// Device destinations of k edge lists (sorted cutoff order).
+struct DevLists {
+  std::vector<int64_t*> src, dst;
+  std::vector<int32_t*> sh;
+};
+
+Status plan_system(const double* pos_host, int64_t n, const double* cell9, const bool pbc[3],
+                   const std::vector<double>& cutoffs, bool disjoint, bool multi,
+                   SystemPlan& sp);
+Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos);
+Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& L,
+                   const int64_t* base, int64_t index_offset);
+
+Status alloc_result(int64_t m, nlb_result* r);
+void zero_results(nlb_result* outs, int32_t k);
+Status empty_results(nlb_result* outs, int32_t k);
+bool cutoffs_valid(const double* cs, int32_t k);
+Status upload_positions(Ctx& c, const double* pos, int64_t n, double** d_pos);
+
+Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_batch,
+                 const double* cutoffs, int32_t k, const double* cells, const uint8_t* pbcs,
+                 const uint8_t* has_cell, int64_t n_cells, bool disjoint, bool multi,
+                 nlb_result* outs);
+
+}  // namespace nlb

@@ -1,0 +1,81 @@
+// nlb_kernels.h -- host launchers for the sm_100a kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "nlb_common.cuh"
+
+namespace nlb {
+
+// ---- k_scan.cu
+// Exclusive scan of n values into out[0..n]; out[n] = total.  `tmp` needs
+// scan_tmp_elems(n) int64 elements.
+int64_t scan_tmp_elems(int64_t n);
+void exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, int64_t* tmp,
+                        cudaStream_t s);
+void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* tmp,
+                        cudaStream_t s);
+
+// ---- k_grid.cu : cell-list build (src/search.rs:92-264)
+// Buffers for one system's grid; all device pointers.
+struct GridBuffers {
+  int32_t* rank_of_bin;   // [total_bins] Morton rank of each linear bin
+  int32_t* bin_count;     // [total_bins] atoms per bin rank (zeroed by caller)
+  int32_t* bin_fill;      // [total_bins] scatter cursors (zeroed by caller)
+  int64_t* bin_start;     // [total_bins + 1]
+  uint64_t* key;          // [n] atom Morton keys (original order)
+  int32_t* rank;          // [n] bin rank of each atom (original order)
+  uint64_t* skey;         // [n] keys scattered by bin
+  int32_t* sidx;          // [n] original indices scattered by bin
+  uint64_t* skey2;        // [n] merge scratch for bins above the shared-memory capacity
+  int32_t* sidx2;         // [n]
+  double* px;             // [n] sorted wrapped positions (SoA)
+  double* py;
+  double* pz;
+  SlotMeta* meta;         // [n] sorted wrap shifts + original index
+  int64_t* scan_tmp;
+};
+
+void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const GridBuffers& b,
+                       cudaStream_t s);
+
+// ---- k_search.cu : count / emit (src/search.rs:291-446, :448-1078, :1187-1405)
+struct CutoffSet {
+  double rc_sq[kMaxCutoffsPerPass];  // ascending squared cutoffs of this pass
+  int32_t k;                         // cutoffs in this pass (1..32)
+  int32_t disjoint;                  // shells: first ascending cutoff only
+  double lower_sq;                   // disjoint: squared cutoff just below this pass (or -1)
+  double max_sq;                     // squared max cutoff of the whole call (pair filter)
+};
+
+struct EmitTargets {
+  int64_t* src[kMaxCutoffsPerPass];  // edge sources per cutoff: [e]
+  int64_t* dst[kMaxCutoffsPerPass];  // edge destinations per cutoff: [e]
+  int32_t* sh[kMaxCutoffsPerPass];   // shifts per cutoff: [3e .. 3e+2]
+  int64_t base[kMaxCutoffsPerPass];  // first edge slot of this system per cutoff
+  int64_t index_offset;              // added to both atom indices (batched systems)
+};
+
+// counts[q * (n + 1) + p] for sorted atom p; the trailing slot of each row is 0.
+void launch_grid_count(const GridParams& g, const GridBuffers& b, int64_t n,
+                       const CutoffSet& cs, uint32_t* counts, cudaStream_t s);
+void launch_grid_emit(const GridParams& g, const GridBuffers& b, int64_t n, const CutoffSet& cs,
+                      const int64_t* offs, const EmitTargets& t, cudaStream_t s);
+
+enum BruteMode : int32_t { kBruteRaw = 0, kBruteMicMode = 1 };
+struct BruteParams {
+  double h[9];
+  double hinv[9];
+  int32_t pbc[3];
+  int32_t mode;
+};
+void launch_brute_count(const BruteParams& bp, const double* pos, int64_t n, const CutoffSet& cs,
+                        uint32_t* counts, cudaStream_t s);
+void launch_brute_emit(const BruteParams& bp, const double* pos, int64_t n, const CutoffSet& cs,
+                       const int64_t* offs, const EmitTargets& t, cudaStream_t s);
+
+// Sets the dynamic shared-memory limit of a kernel once per device.
+void ensure_smem_attr(const void* func, int bytes);
+
+}  // namespace nlb

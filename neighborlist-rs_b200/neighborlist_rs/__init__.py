@@ -1,0 +1,395 @@
+"""neighborlist_rs -- B200 drop-in for the Python module of solccp/neighborlist-rs.
+
+Same functions, signatures, defaults, dict layout, dtypes and ValueError
+messages as the reference's PyO3 module (src/python_api.rs:15-626,
+neighborlist_rs.pyi); the search itself runs in the CUDA library
+``_lib/libnlb200.so`` (C ABI: include/neighborlist_b200.h).  There is no CPU
+fallback: importing this module fails if the library is missing, and every
+build call fails if no CUDA device is available.
+
+Results are numpy arrays that view pinned host memory owned by the library;
+the memory is returned to the library when the arrays are garbage-collected.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import weakref
+
+import numpy as np
+
+__all__ = [
+    "PyCell", "build_neighborlists", "build_from_ase", "build_neighborlists_multi",
+    "build_multi_from_ase", "build_neighborlists_batch", "build_neighborlists_batch_multi",
+    "get_num_threads", "set_num_threads", "init_logging", "get_brute_force_threshold",
+    "set_brute_force_threshold", "get_parallel_threshold", "set_parallel_threshold",
+    "get_stack_threshold", "set_stack_threshold",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libnlb200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"neighborlist_rs: CUDA library not found at {LIB_PATH}; build it with "
+        "`python neighborlist-rs_b200/build.py` (nvcc, sm_100a)")
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("n_edges", ctypes.c_int64),
+                ("edge_index", ctypes.c_void_p),
+                ("shift", ctypes.c_void_p)]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+_lib = ctypes.CDLL(LIB_PATH)
+_lib.nlb_last_error.restype = ctypes.c_char_p
+_lib.nlb_version.restype = ctypes.c_char_p
+_lib.nlb_build.argtypes = [_dp, ctypes.c_int64, ctypes.c_double, _dp, _u8p, ctypes.c_int,
+                           ctypes.POINTER(_Result)]
+_lib.nlb_build_multi.argtypes = [_dp, ctypes.c_int64, _dp, ctypes.c_int32, _dp, _u8p,
+                                 ctypes.c_int, ctypes.POINTER(_Result)]
+_lib.nlb_build_batch.argtypes = [_dp, ctypes.c_int64, _i32p, ctypes.c_int64, ctypes.c_double,
+                                 _dp, _u8p, _u8p, ctypes.c_int64, ctypes.c_int,
+                                 ctypes.POINTER(_Result)]
+_lib.nlb_build_batch_multi.argtypes = [_dp, ctypes.c_int64, _i32p, ctypes.c_int64, _dp,
+                                       ctypes.c_int32, _dp, _u8p, _u8p, ctypes.c_int64,
+                                       ctypes.c_int, ctypes.POINTER(_Result)]
+_lib.nlb_result_free.argtypes = [ctypes.POINTER(_Result)]
+_lib.nlb_host_free.argtypes = [ctypes.c_void_p]
+_lib.nlb_cell_check.argtypes = [_dp]
+_lib.nlb_cell_wrap.argtypes = [_dp, _u8p, _dp, _dp]
+for _name in ("brute_force", "parallel", "stack"):
+    getattr(_lib, f"nlb_get_{_name}_threshold").restype = ctypes.c_size_t
+    getattr(_lib, f"nlb_set_{_name}_threshold").argtypes = [ctypes.c_size_t]
+
+_NLB_ERR_VALUE = 1
+_LOG_LEVEL = None
+
+
+def _check(code: int) -> None:
+    if code == 0:
+        return
+    msg = _lib.nlb_last_error().decode()
+    if code == _NLB_ERR_VALUE:
+        raise ValueError(msg)
+    raise RuntimeError(f"neighborlist_rs (CUDA): {msg}")
+
+
+def _arr(ptr, count, ctype, dtype):
+    """numpy view of `count` library-owned elements; freed with the array."""
+    if count == 0:
+        _lib.nlb_host_free(ptr)
+        return np.zeros(0, dtype=dtype)
+    buf = (ctype * count).from_address(ptr)
+    weakref.finalize(buf, _lib.nlb_host_free, ctypes.c_void_p(ptr))
+    return np.frombuffer(buf, dtype=dtype)
+
+
+def _to_dict(r: _Result) -> dict:
+    m = int(r.n_edges)
+    ei = _arr(r.edge_index, 2 * m, ctypes.c_int64, np.int64).reshape(2, m)
+    sh = _arr(r.shift, 3 * m, ctypes.c_int32, np.int32).reshape(m, 3)
+    return {"edge_index": ei, "shift": sh}
+
+
+def _empty() -> dict:
+    return {"edge_index": np.zeros((2, 0), np.int64), "shift": np.zeros((0, 3), np.int32)}
+
+
+def _positions(positions) -> np.ndarray:
+    # PyReadonlyArray2<f64> (src/python_api.rs:116-137): a 2-D float64 array,
+    # copied when not C-contiguous.
+    if not isinstance(positions, np.ndarray) or positions.ndim != 2 or positions.dtype != np.float64:
+        raise TypeError("positions must be a 2-D numpy array of float64")
+    if positions.shape[1] != 3:
+        raise ValueError("Positions must be (N, 3)")
+    return np.ascontiguousarray(positions)
+
+
+def _batch_ids(batch) -> np.ndarray:
+    if not isinstance(batch, np.ndarray) or batch.ndim != 1 or batch.dtype != np.int32:
+        raise TypeError("batch must be a 1-D numpy array of int32")
+    return np.ascontiguousarray(batch)
+
+
+def _check_cutoff(cutoff) -> float:
+    c = float(cutoff)
+    if not math.isfinite(c) or c <= 0.0:
+        raise ValueError("Cutoff must be positive and finite")
+    return c
+
+
+def _cutoff_list(cutoffs) -> list:
+    if isinstance(cutoffs, (str, bytes)):
+        raise TypeError("cutoffs must be a sequence of floats")
+    return [float(c) for c in cutoffs]
+
+
+def _rust_float(x: float) -> str:
+    """Rust's Display for f64 (shortest round-trip digits, never an exponent)."""
+    if math.isnan(x):
+        return "NaN"
+    if math.isinf(x):
+        return "inf" if x > 0 else "-inf"
+    return np.format_float_positional(x, trim="-")
+
+
+class PyCell:
+    """Simulation cell (src/python_api.rs:15-99).
+
+    ``h`` is a 3x3 nested list whose COLUMNS are the lattice vectors (the
+    reference feeds it to ``Matrix3::new`` row by row); ``pbc`` defaults to
+    all periodic.  ``from_ase`` transposes an ASE cell (rows = vectors).
+    """
+
+    __slots__ = ("_h9", "_pbc")
+
+    def __init__(self, h, pbc=None):
+        rows = [list(r) for r in h] if not isinstance(h, (str, bytes)) else []
+        if len(rows) != 3 or any(len(r) != 3 for r in rows):
+            raise ValueError("Cell matrix must be 3x3")
+        self._h9 = np.ascontiguousarray(np.array(rows, dtype=np.float64).reshape(9))
+        if pbc is None:
+            pbc = (True, True, True)
+        p = [bool(x) for x in pbc]
+        if len(p) != 3:
+            raise ValueError("pbc must have 3 entries")
+        self._pbc = np.ascontiguousarray(np.array(p, dtype=np.uint8))
+        _check(_lib.nlb_cell_check(self._h9.ctypes.data_as(_dp)))
+
+    def wrap(self, pos):
+        p = np.ascontiguousarray(np.array([float(x) for x in pos], dtype=np.float64))
+        if p.shape != (3,):
+            raise ValueError("pos must have 3 entries")
+        out = np.zeros(3, np.float64)
+        _check(_lib.nlb_cell_wrap(self._h9.ctypes.data_as(_dp), self._pbc.ctypes.data_as(_u8p),
+                                  p.ctypes.data_as(_dp), out.ctypes.data_as(_dp)))
+        return [float(v) for v in out]
+
+    def __repr__(self):
+        h = [_rust_float(float(v)) for v in self._h9]
+        pb = ["true" if v else "false" for v in self._pbc]
+        return (f"PyCell(h=[[{h[0]}, {h[1]}, {h[2]}], [{h[3]}, {h[4]}, {h[5]}], "
+                f"[{h[6]}, {h[7]}, {h[8]}]], pbc=[{pb[0]}, {pb[1]}, {pb[2]}])")
+
+    @staticmethod
+    def from_ase(atoms) -> "PyCell":
+        c = np.asarray(atoms.get_cell().__array__(), dtype=np.float64)
+        if c.shape != (3, 3):
+            raise ValueError("Cell must be 3x3")
+        pbc = [bool(x) for x in atoms.get_pbc()]
+        return PyCell(c.T.tolist(), pbc)
+
+
+def _cell_args(cell):
+    if cell is None:
+        return None, None
+    if not isinstance(cell, PyCell):
+        raise TypeError("cell must be a PyCell or None")
+    return cell._h9.ctypes.data_as(_dp), cell._pbc.ctypes.data_as(_u8p)
+
+
+def build_neighborlists(cell, positions, cutoff, parallel=True):
+    """src/python_api.rs:139-186.  Half list (i < j, or i == j with a non-zero
+    image); returns {"edge_index": int64 (2, M), "shift": int32 (M, 3)}."""
+    c = _check_cutoff(cutoff)
+    pos = _positions(positions)
+    n = pos.shape[0]
+    if n == 0:
+        return _empty()
+    h, pb = _cell_args(cell)
+    r = _Result()
+    _check(_lib.nlb_build(pos.ctypes.data_as(_dp), n, c, h, pb, int(bool(parallel)),
+                          ctypes.byref(r)))
+    return _to_dict(r)
+
+
+def _ase_inputs(atoms):
+    # src/python_api.rs:188-209
+    positions = atoms.get_positions()
+    pbc = [bool(x) for x in atoms.get_pbc()]
+    cell = PyCell.from_ase(atoms) if any(pbc) else None
+    return positions, cell
+
+
+def build_from_ase(atoms, cutoff):
+    """src/python_api.rs:211-220."""
+    positions, cell = _ase_inputs(atoms)
+    return build_neighborlists(cell, positions, cutoff, True)
+
+
+def _multi_dict(results, labels):
+    out = {}
+    for k, r in enumerate(results):
+        out[labels[k] if labels is not None else k] = r
+    return out
+
+
+def build_neighborlists_multi(cell, positions, cutoffs, labels=None, disjoint=False):
+    """src/python_api.rs:235-309.  One traversal for all cutoffs; returns a
+    dict keyed by cutoff index (or label)."""
+    pos = _positions(positions)
+    cs = _cutoff_list(cutoffs)
+    if not cs:
+        return {}
+    if any(not math.isfinite(c) or c <= 0.0 for c in cs):
+        raise ValueError("All cutoffs must be positive and finite")
+    if labels is not None:
+        labels = [str(x) for x in labels]
+        if len(labels) != len(cs):
+            raise ValueError("Length of labels must match length of cutoffs")
+    n = pos.shape[0]
+    if n == 0:
+        return _multi_dict([_empty() for _ in cs], labels)
+    h, pb = _cell_args(cell)
+    k = len(cs)
+    carr = np.ascontiguousarray(np.array(cs, dtype=np.float64))
+    outs = (_Result * k)()
+    _check(_lib.nlb_build_multi(pos.ctypes.data_as(_dp), n, carr.ctypes.data_as(_dp), k, h, pb,
+                                int(bool(disjoint)), outs))
+    return _multi_dict([_to_dict(outs[q]) for q in range(k)], labels)
+
+
+def build_multi_from_ase(atoms, cutoffs, labels=None, disjoint=False):
+    """src/python_api.rs:222-233."""
+    positions, cell = _ase_inputs(atoms)
+    return build_neighborlists_multi(cell, positions, cutoffs, labels, disjoint)
+
+
+def _batch_cells(cells, batch):
+    """Monotonic check, system count and the (B,3,3) cells -> C arrays
+    (src/python_api.rs:353-407): a zero matrix means isolated (auto-box); any
+    other cell is transposed from ASE rows and gets pbc (T, T, T)."""
+    n_sys = 1
+    cur = int(batch[0])
+    # vectorised form of the reference's scan
+    d = np.diff(batch.astype(np.int64))
+    if (d < 0).any():
+        raise ValueError("Batch IDs must be monotonic (non-decreasing)")
+    n_sys = 1 + int((d != 0).sum())
+    del cur
+    if cells is None:
+        return n_sys, None, None, None, 0
+    if not isinstance(cells, np.ndarray) or cells.ndim != 3 or cells.dtype != np.float64:
+        raise TypeError("cells must be a 3-D numpy array of float64")
+    if cells.shape[0] < n_sys:
+        raise ValueError(f"Expected at least {n_sys} cells, but got {cells.shape[0]}")
+    c = np.asarray(cells[:n_sys])
+    if c.shape[1:] != (3, 3):
+        raise ValueError("cells must have shape (B, 3, 3)")
+    has = np.any(c != 0.0, axis=(1, 2)).astype(np.uint8)
+    h9 = np.ascontiguousarray(np.transpose(c, (0, 2, 1)).reshape(n_sys, 9))
+    pbcs = np.ones((n_sys, 3), np.uint8)
+    return n_sys, h9, pbcs, has, n_sys
+
+
+def build_neighborlists_batch(positions, batch, cells=None, cutoff=5.0, parallel=True):
+    """src/python_api.rs:315-423.  Systems split wherever the batch id
+    changes; indices are global; systems concatenated in order."""
+    c = _check_cutoff(cutoff)
+    pos = _positions(positions)
+    b = _batch_ids(batch)
+    n = pos.shape[0]
+    if b.shape[0] != n:
+        raise ValueError("positions and batch must have the same length")
+    if n == 0:
+        return _empty()
+    _, h9, pbcs, has, nc = _batch_cells(cells, b)
+    r = _Result()
+    _check(_lib.nlb_build_batch(
+        pos.ctypes.data_as(_dp), n, b.ctypes.data_as(_i32p), n, c,
+        h9.ctypes.data_as(_dp) if h9 is not None else None,
+        pbcs.ctypes.data_as(_u8p) if pbcs is not None else None,
+        has.ctypes.data_as(_u8p) if has is not None else None, nc, int(bool(parallel)),
+        ctypes.byref(r)))
+    return _to_dict(r)
+
+
+def build_neighborlists_batch_multi(positions, batch, cells=None, cutoffs=(5.0,), labels=None,
+                                    disjoint=False):
+    """src/python_api.rs:425-546."""
+    pos = _positions(positions)
+    b = _batch_ids(batch)
+    n = pos.shape[0]
+    if b.shape[0] != n:
+        raise ValueError("positions and batch must have the same length")
+    cs = _cutoff_list(cutoffs)
+    if n == 0 or not cs:
+        return {}
+    if any(not math.isfinite(c) or c <= 0.0 for c in cs):
+        raise ValueError("All cutoffs must be positive and finite")
+    if labels is not None:
+        labels = [str(x) for x in labels]
+        if len(labels) != len(cs):
+            raise ValueError("Length of labels must match length of cutoffs")
+    _, h9, pbcs, has, nc = _batch_cells(cells, b)
+    k = len(cs)
+    carr = np.ascontiguousarray(np.array(cs, dtype=np.float64))
+    outs = (_Result * k)()
+    _check(_lib.nlb_build_batch_multi(
+        pos.ctypes.data_as(_dp), n, b.ctypes.data_as(_i32p), n, carr.ctypes.data_as(_dp), k,
+        h9.ctypes.data_as(_dp) if h9 is not None else None,
+        pbcs.ctypes.data_as(_u8p) if pbcs is not None else None,
+        has.ctypes.data_as(_u8p) if has is not None else None, nc, int(bool(disjoint)), outs))
+    return _multi_dict([_to_dict(outs[q]) for q in range(k)], labels)
+
+
+# ---------------------------------------------------------------- configuration
+
+def get_num_threads() -> int:
+    """The reference reports its rayon pool size; the device path has no host
+    thread pool, so this reports the host's logical CPU count (rayon's default)."""
+    return os.cpu_count() or 1
+
+
+def set_num_threads(n) -> None:
+    """Accepted for API parity (src/python_api.rs:553-561); no effect on the GPU path."""
+    int(n)
+
+
+def init_logging(level=None) -> None:
+    """src/python_api.rs:593-605.  Records the level; the library reports
+    per-phase timings through bench.py / ncu rather than tracing spans."""
+    global _LOG_LEVEL
+    _LOG_LEVEL = level if level is not None else "info"
+
+
+def _usize(val) -> int:
+    v = int(val)
+    if v < 0:
+        raise OverflowError("can't convert negative int to unsigned")
+    return v
+
+
+def get_brute_force_threshold() -> int:
+    return int(_lib.nlb_get_brute_force_threshold())
+
+
+def set_brute_force_threshold(val) -> None:
+    _lib.nlb_set_brute_force_threshold(_usize(val))
+
+
+def get_parallel_threshold() -> int:
+    return int(_lib.nlb_get_parallel_threshold())
+
+
+def set_parallel_threshold(val) -> None:
+    _lib.nlb_set_parallel_threshold(_usize(val))
+
+
+def get_stack_threshold() -> int:
+    return int(_lib.nlb_get_stack_threshold())
+
+
+def set_stack_threshold(val) -> None:
+    _lib.nlb_set_stack_threshold(_usize(val))
+
+
+def version() -> str:
+    return _lib.nlb_version().decode()

@@ -1,0 +1,208 @@
+"""Parity of the CUDA library (through the drop-in Python API and the C ABI)
+with the CPU oracle: identical edge_index and shift arrays, element by
+element and in the same order (integer index work: bit-exact)."""
+
+import numpy as np
+import pytest
+
+from helpers import assert_same
+
+pytestmark = pytest.mark.gpu
+
+PBC3 = [True, True, True]
+
+
+@pytest.fixture(scope="module")
+def nl():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import neighborlist_rs
+
+    return neighborlist_rs
+
+
+def eye(s):
+    return np.eye(3) * s
+
+
+def single(nl, oracle, pos, h, rc, pbc=PBC3, what=""):
+    cell = None if h is None else nl.PyCell(np.asarray(h).tolist(), pbc)
+    got = nl.build_neighborlists(cell, np.ascontiguousarray(pos, dtype=np.float64), rc)
+    ref = oracle.search_single(pos, h, None if h is None else pbc, rc, nthreads=8)
+    assert_same(got, ref, what)
+    return got
+
+
+# ---------------------------------------------------------------- fixtures
+
+@pytest.mark.parametrize("rc", [6.0, 14.0])
+@pytest.mark.parametrize("name", ["isolated_100", "isolated_two_clusters", "isolated_1000",
+                                  "isolated_10000", "ethanol_1000", "ethanol_10000", "si_bulk"])
+def test_fixture_parity(nl, oracle, fixtures, golden_counts, name, rc):
+    pos, rows = fixtures[name]
+    got = single(nl, oracle, pos, None if rows is None else rows.T, rc, what=f"{name} rc {rc}")
+    ei = got["edge_index"]
+    assert int((ei[0] != ei[1]).sum()) == golden_counts[str(rc)][name]["edges_i_ne_j"]
+
+
+# ---------------------------------------------------------------- synthetic workloads
+
+def test_isolated_cube_1000(nl, oracle):
+    from neighborlist_rs import workloads as W
+
+    single(nl, oracle, W.isolated_cube(), None, 6.0, what="isolated cube N=1000 rc 6")
+
+
+@pytest.mark.parametrize("rc", [6.0, 14.0])
+def test_cluster_liquid(nl, oracle, rc):
+    from neighborlist_rs import workloads as W
+
+    pos, rows = W.cluster_liquid()
+    single(nl, oracle, pos, rows.T, rc, what=f"cluster liquid rc {rc}")
+
+
+def test_triclinic_multi(nl, oracle):
+    from neighborlist_rs import workloads as W
+
+    pos, rows = W.triclinic_uniform()
+    cell = nl.PyCell(rows.T.tolist())
+    got = nl.build_neighborlists_multi(cell, pos, [5.0, 6.0, 12.0])
+    ref = oracle.search_single_multi(pos, rows.T, PBC3, [5.0, 6.0, 12.0], nthreads=8)
+    for q in range(3):
+        assert_same(got[q], ref[q], f"triclinic multi cutoff {q}")
+
+
+# ---------------------------------------------------------------- paths and edge cases
+
+def test_empty_and_single_atom(nl, oracle):
+    r = nl.build_neighborlists(None, np.zeros((0, 3)), 3.0)
+    assert r["edge_index"].shape == (2, 0) and r["shift"].shape == (0, 3)
+    single(nl, oracle, np.zeros((1, 3)), eye(5.0), 6.0, what="self images")
+    single(nl, oracle, np.zeros((1, 3)), None, 6.0, what="single isolated atom")
+
+
+def test_many_images_tiny_box(nl, oracle):
+    # src/search.rs:1860-1882: rc 10 in a 1 A box (21 images per axis)
+    single(nl, oracle, np.array([[0.5, 0.5, 0.5]]), eye(1.0), 10.0, what="rc 10 in 1 A box")
+    rng = np.random.default_rng(7)
+    h = np.array([[4.0, 1.0, 0.5], [0.0, 3.5, -0.8], [0.0, 0.0, 3.0]])
+    pos = rng.random((40, 3)) @ h.T
+    single(nl, oracle, pos, h, 7.5, what="small triclinic box, many images")
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_brute_force_paths(nl, oracle, seed):
+    rng = np.random.default_rng(100 + seed)
+    n = int(rng.integers(2, 900))
+    side = (n / 0.1) ** (1 / 3)
+    pos = rng.random((n, 3)) * side
+    single(nl, oracle, pos, None, 5.0, what="brute isolated")
+    L = max(side, 11.0)
+    single(nl, oracle, pos, eye(L), 5.0, what="brute MIC")
+    h = np.array([[L, 0.3 * L, 0.1 * L], [0.0, L, 0.2 * L], [0.0, 0.0, L]])
+    single(nl, oracle, pos @ np.array(h).T / L, h, 4.0, what="brute MIC triclinic")
+    single(nl, oracle, pos, eye(L), 5.0, pbc=[True, False, True], what="brute MIC mixed pbc")
+
+
+def test_threshold_changes_dispatch(nl, oracle):
+    pos = np.random.default_rng(3).random((200, 3)) * 12.0
+    old = nl.get_brute_force_threshold()
+    nl.set_brute_force_threshold(0)
+    oracle.set_thresholds(0, 300)
+    try:
+        single(nl, oracle, pos, None, 3.0, what="cell list forced (isolated)")
+        single(nl, oracle, pos, eye(12.0), 3.0, what="cell list forced (pbc)")
+        single(nl, oracle, pos, eye(12.0), 3.0, pbc=[True, False, False], what="Q1 mixed pbc")
+    finally:
+        nl.set_brute_force_threshold(old)
+        oracle.set_thresholds(1000, 300)
+
+
+def test_duplicates_and_boundaries(nl, oracle):
+    rng = np.random.default_rng(11)
+    base = rng.random((600, 3)) * 20.0
+    pos = np.concatenate([base, base[:300], np.zeros((50, 3)), np.full((50, 3), 20.0),
+                          np.full((30, 3), -20.0), np.full((30, 3), 40.0 - 1e-12)])
+    single(nl, oracle, pos, eye(20.0), 4.0, what="duplicates / boundaries / outside")
+    single(nl, oracle, pos, None, 4.0, what="duplicates isolated")
+
+
+def test_large_bin_merge_path(nl, oracle):
+    # A single bin of 3000 atoms exercises the merge path of the bin sort.
+    pos = np.random.default_rng(5).random((3000, 3)) * 8.0
+    single(nl, oracle, pos, eye(8.0), 4.5, what="one 3000-atom bin")
+
+
+def test_multi_cutoff_variants(nl, oracle, fixtures):
+    pos, rows = fixtures["ethanol_1000"]
+    cell = nl.PyCell(rows.T.tolist())
+    for cs, dj in [([6.0, 3.0, 4.5], False), ([6.0, 3.0, 4.5], True), ([3.0, 3.0], True)]:
+        got = nl.build_neighborlists_multi(cell, pos, cs, disjoint=dj)
+        ref = oracle.search_single_multi(pos, rows.T, PBC3, cs, disjoint=dj, nthreads=8)
+        for q in range(len(cs)):
+            assert_same(got[q], ref[q], f"multi {cs} disjoint={dj} q={q}")
+    # more than one 32-cutoff pass, with disjoint shells across the pass boundary
+    cs = list(np.linspace(1.0, 7.0, 45))
+    for dj in (False, True):
+        got = nl.build_neighborlists_multi(cell, pos, cs, disjoint=dj)
+        ref = oracle.search_single_multi(pos, rows.T, PBC3, cs, disjoint=dj, nthreads=8)
+        for q in range(len(cs)):
+            assert_same(got[q], ref[q], f"45 cutoffs disjoint={dj} q={q}")
+
+
+def test_multi_brute_and_labels(nl, oracle):
+    pos = np.array([[0.0, 0, 0], [1.0, 0, 0], [2.5, 0, 0]])
+    got = nl.build_neighborlists_multi(None, pos, [1.6, 3.0], labels=["s", "l"])
+    ref = oracle.search_single_multi(pos, None, None, [1.6, 3.0])
+    assert_same(got["s"], ref[0], "labels s")
+    assert_same(got["l"], ref[1], "labels l")
+
+
+def test_batch_parity(nl, oracle):
+    from neighborlist_rs import workloads as W
+
+    systems = W.uneven_batch(n_systems=96)
+    pos, batch, cells = W.concat_batch(systems)
+    got = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=5.0)
+    ocells = [None if not c.any() else (c.T, PBC3) for c in cells]
+    (ref,) = oracle.search_batch(pos, batch, ocells, [5.0], nthreads=8)
+    assert_same(got, ref, "uneven batch")
+    gm = nl.build_neighborlists_batch_multi(pos, batch, cells=cells, cutoffs=[5.0, 3.0])
+    refm = oracle.search_batch(pos, batch, ocells, [5.0, 3.0], nthreads=8)
+    assert_same(gm[0], refm[0], "batch multi 5")
+    assert_same(gm[1], refm[1], "batch multi 3")
+
+
+def test_batch_matches_singles(nl):
+    """tests/test_batch.py:68-120: each system of a batch equals its single call."""
+    from neighborlist_rs import workloads as W
+
+    systems = W.uneven_batch(n_systems=12, seed=9)
+    pos, batch, cells = W.concat_batch(systems)
+    got = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=5.0)
+    start = 0
+    parts = []
+    for s in systems:
+        cell = None if s.cell_rows is None else nl.PyCell(s.cell_rows.T.tolist())
+        r = nl.build_neighborlists(cell, s.positions, 5.0)
+        parts.append((r["edge_index"] + start, r["shift"]))
+        start += len(s.positions)
+    ei = np.concatenate([p[0] for p in parts], axis=1)
+    sh = np.concatenate([p[1] for p in parts], axis=0)
+    assert np.array_equal(got["edge_index"], ei) and np.array_equal(got["shift"], sh)
+
+
+def test_non_contiguous_inputs(nl):
+    # tests/test_memory_layout.py
+    rng = np.random.default_rng(0)
+    pos = rng.random((100, 3)) * 10.0
+    big = np.zeros((100, 4))
+    big[:, :3] = pos
+    a = nl.build_neighborlists(None, pos, 1.5)
+    b = nl.build_neighborlists(None, big[:, :3], 1.5)
+    assert np.array_equal(a["edge_index"], b["edge_index"])
+    bl = np.zeros(200, np.int32)
+    r = nl.build_neighborlists_batch(big[:50, :3], bl[::2][:50], None, 1.5)
+    assert r["edge_index"].shape[0] == 2
