@@ -1,0 +1,422 @@
+"""Benchmark of the B200 neighbour-list engine (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Headline workload: the periodic cluster liquid (1112 rigid 9-atom clusters,
+N = 10,008, cubic L = 46.4 A, full PBC) at rc = 6 A; one step = one complete
+neighbour-list build of that system (cell list build, count, scan, emit of the
+exact-sized edge_index int64 (2, M) and shift int32 (M, 3)).
+
+* value      : edges/s over all ranks, device-resident: positions already in
+               HBM, edge arrays left in HBM (nlb_build_device); CUDA events on
+               the launching stream around each step; L2 flushed (256 MB write)
+               between steps, outside the timed spans.
+* e2e        : same metric through the reference-facing call with host buffers
+               (neighborlist_rs.build_neighborlists: numpy positions in, numpy
+               edge arrays out), host<->device copies inside the timed region.
+* roofline   : the dominant kernel's algorithmic bytes / its CUDA-event time.
+* cpu_baseline: the CPU oracle (C++ restatement of the reference's rayon
+               count/fill path) on the host cores, rank 0, bounded sample.
+* extra      : other configurations (rc 14, isolated N=1000, triclinic
+               multi-cutoff, batched uneven systems) measured the same way.
+
+Multi-GPU: systems are independent, so each rank builds its own copy of the
+workload (weak scaling, no collective on the data path); the step time is the
+max over ranks.  `--impl reference` times the CPU oracle on all host threads
+(rank 0 only).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "neighborlist-rs_b200")
+for _p in (ROOT, PKG_DIR):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "edges/s (exact edges; cluster-liquid N=10008 PBC rc=6)"
+UNIT = "edges/s"
+WORKLOAD = "cluster_liquid N=10008 (1112 x 9-atom clusters) cubic L=46.4 A full PBC rc=6.0 A"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-extra", action="store_true", help="headline workload only")
+    ap.add_argument("--rc", type=float, default=6.0,
+                    help="cutoff of the timed workload (6.0 = headline; 14.0 for profiling)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+
+def dist_init(backend):
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and not dist.is_initialized():
+        import datetime
+
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, local, world
+
+
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workloads
+
+def headline_system():
+    from neighborlist_rs import workloads as W
+
+    pos, rows = W.cluster_liquid()
+    return pos, rows
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- device timing
+
+class DeviceTimer:
+    """Times device-resident builds of one system with CUDA events on the
+    stream the library launches on; L2 flushed between steps."""
+
+    def __init__(self, nl, torch, pos, rows, rc):
+        self.nl, self.torch = nl, torch
+        self.cell = None if rows is None else nl.PyCell(rows.T.tolist())
+        self.dpos = torch.from_numpy(np.ascontiguousarray(pos)).cuda()
+        self.n = pos.shape[0]
+        self.rc = rc
+        self.flush = torch.empty(256 << 20, dtype=torch.int8, device="cuda")
+        # A dedicated (non-default) stream: the library launches on it and the
+        # timing events are recorded on it.
+        self.stream = torch.cuda.Stream()
+        nl.set_stream(self.stream.cuda_stream)
+
+    def step(self):
+        return self.nl.build_device_raw(self.cell, self.dpos.data_ptr(), self.n, self.rc)[0]
+
+    def run(self, steps, warmup):
+        torch = self.torch
+        for _ in range(warmup):
+            self.step()
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        edges = 0
+        l0 = self.nl.kernel_launches()
+        for k in range(steps):
+            with torch.cuda.stream(self.stream):
+                self.flush.zero_()
+            starts[k].record(self.stream)
+            edges += self.step()
+            ends[k].record(self.stream)
+        torch.cuda.synchronize()
+        launches = self.nl.kernel_launches() - l0
+        ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+        self.nl.set_stream(self.stream.cuda_stream)
+        return ms, edges, launches
+
+    def phases(self, steps):
+        self.nl.profile(True)
+        for _ in range(steps):
+            with self.torch.cuda.stream(self.stream):
+                self.flush.zero_()
+            self.step()
+        self.torch.cuda.synchronize()
+        calls, ph = self.nl.profile_read()
+        self.nl.profile(False)
+        return {k: v / max(calls, 1) for k, v in ph.items()}
+
+
+def e2e_time(nl, pos, rows, rc, steps, warmup):
+    cell = None if rows is None else nl.PyCell(rows.T.tolist())
+    for _ in range(warmup):
+        nl.build_neighborlists(cell, pos, rc)
+    t = 0.0
+    m = 0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        r = nl.build_neighborlists(cell, pos, rc)
+        t += time.perf_counter() - t0
+        m = r["edge_index"].shape[1]
+        del r
+    return t, m
+
+
+def cpu_oracle_time(pos, rows, rc, budget_s=4.0, min_reps=15, threads=None):
+    import oracle
+
+    threads = threads or (os.cpu_count() or 1)
+    h = None if rows is None else rows.T
+    pbc = None if rows is None else [True] * 3
+    for _ in range(2):
+        ei, _ = oracle.search_single(pos, h, pbc, rc, nthreads=threads)
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < min_reps or time.perf_counter() - t_start < budget_s:
+        t0 = time.perf_counter()
+        ei, _ = oracle.search_single(pos, h, pbc, rc, nthreads=threads)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > 3 * budget_s:
+            break
+    return statistics.mean(times), ei.shape[1], threads, len(times)
+
+
+# ---------------------------------------------------------------- arms
+
+def run_reference(args):
+    rank, _, world = dist_init("gloo")
+    if rank != 0:
+        return
+    pos, rows = headline_system()
+    import oracle
+
+    threads = os.cpu_count() or 1
+    h, pbc = rows.T, [True] * 3
+    for _ in range(args.warmup):
+        oracle.search_single(pos, h, pbc, 6.0, nthreads=threads)
+    t = 0.0
+    m = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ei, _ = oracle.search_single(pos, h, pbc, 6.0, nthreads=threads)
+        t += time.perf_counter() - t0
+        m = ei.shape[1]
+    value = m * args.steps / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "edges_per_step": m, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full builds of the workload (C++ restatement "
+                                   "of the reference rayon count/fill path; the Rust crate "
+                                   "cannot be built here)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+
+    rank, local, world = dist_init("nccl")
+    torch.cuda.set_device(local)
+    import neighborlist_rs as nl
+
+    pos, rows = headline_system()
+    n = pos.shape[0]
+    dt = DeviceTimer(nl, torch, pos, rows, args.rc)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ms, edges, launches = dt.run(args.steps, args.warmup)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_max = max_over_ranks(ms, world, "cuda")
+    m_step = edges // args.steps
+    value = edges * world / (ms_max * 1e-3)
+
+    # per-phase CUDA-event times -> roofline of the dominant kernel
+    ph = dt.phases(max(5, args.steps // 3))
+    peak, peak_kind = peaks()
+    bytes_emit = 28 * m_step + 48 * n      # edge_index + shift writes; sorted SoA + offsets read
+    bytes_count = 44 * n                   # sorted SoA read, counts written
+    dominant = "emit" if ph["emit"] >= ph["count"] else "count"
+    alg = bytes_emit if dominant == "emit" else bytes_count
+    achieved = alg / (ph[dominant] * 1e-3) / 1e9
+    kernel_name = {"emit": "k_grid_emit", "count": "k_grid_count"}[dominant]
+
+    # e2e through the reference-facing call (host buffers)
+    nl.set_stream(None)
+    t_e2e, m_e2e = e2e_time(nl, pos, rows, args.rc, args.steps, args.warmup)
+    e2e_value = m_e2e * args.steps * world / max_over_ranks(t_e2e, world, "cuda")
+
+    metric, workload = METRIC, WORKLOAD
+    if args.rc != 6.0:
+        metric = METRIC.replace("rc=6", f"rc={args.rc:g}")
+        workload = WORKLOAD.replace("rc=6.0", f"rc={args.rc:g}")
+    line = {
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded cluster liquid)",
+        "config": {"workload": workload, "atoms": n, "edges_per_step": m_step,
+                   "parallelism": f"replicas x{world} (independent systems)",
+                   "l2": "flushed between steps (256 MB write)"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "algorithmic_bytes": alg, "kernel_ms": ph[dominant], "traffic": None,
+                     "phases_ms": ph},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n + 72,
+                "d2h_bytes_per_step": 28 * m_e2e},
+    }
+    if rank == 0:
+        t_cpu, m_cpu, threads, reps = cpu_oracle_time(pos, rows, args.rc)
+        line["cpu_baseline"] = {
+            "value": m_cpu / t_cpu, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{reps} full builds of the workload (mean), C++ restatement of the "
+                      "reference's rayon count/fill path"}
+        if not args.no_extra:
+            line["extra"] = extra_measurements(nl, torch, args)
+        print(json.dumps(line), flush=True)
+    barrier(world)
+
+
+def extra_measurements(nl, torch, args):
+    from neighborlist_rs import workloads as W
+
+    out = {}
+    steps = max(5, args.steps // 3)
+    pos, rows = headline_system()
+    dt = DeviceTimer(nl, torch, pos, rows, 14.0)
+    ms, edges, _ = dt.run(steps, 2)
+    out["cluster_liquid_rc14"] = {"edges_per_s": edges / (ms * 1e-3), "ms_per_step": ms / steps,
+                                  "edges": edges // steps}
+    p1 = W.isolated_cube()
+    dt = DeviceTimer(nl, torch, p1, None, 6.0)
+    ms, edges, _ = dt.run(steps, 2)
+    out["isolated_cube_1000_rc6"] = {"edges_per_s": edges / (ms * 1e-3),
+                                     "ms_per_step": ms / steps, "edges": edges // steps}
+    nl.set_stream(None)
+    # triclinic multi-cutoff (host-buffer call)
+    p3, r3 = W.triclinic_uniform()
+    cell = nl.PyCell(r3.T.tolist())
+    nl.build_neighborlists_multi(cell, p3, [5.0, 6.0, 12.0])
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        r = nl.build_neighborlists_multi(cell, p3, [5.0, 6.0, 12.0])
+    dtm = (time.perf_counter() - t0) / reps
+    m3 = sum(v["edge_index"].shape[1] for v in r.values())
+    out["triclinic_multi_e2e"] = {"edges_per_s": m3 / dtm, "ms_per_call": 1e3 * dtm,
+                                  "edges": m3}
+    # batched uneven systems (host-buffer call)
+    systems = W.uneven_batch()
+    pb, bb, cb = W.concat_batch(systems)
+    nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0)
+    t0 = time.perf_counter()
+    rb = nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0)
+    dtb = time.perf_counter() - t0
+    out["uneven_batch_4096_e2e"] = {"systems_per_s": len(systems) / dtb,
+                                    "edges_per_s": rb["edge_index"].shape[1] / dtb,
+                                    "ms_per_call": 1e3 * dtb, "atoms": int(pb.shape[0]),
+                                    "edges": int(rb["edge_index"].shape[1])}
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as dist
+
+        if dist.is_initialized():
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

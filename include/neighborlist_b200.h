@@ -96,6 +96,40 @@ void nlb_set_parallel_threshold(size_t v);
 size_t nlb_get_stack_threshold(void);
 void nlb_set_stack_threshold(size_t v);
 
+/* ---- Device-resident path (positions and results stay in HBM). ----
+ * nlb_build_device: like nlb_build, but `d_positions` is a device pointer and
+ * the result arrays are device pointers into the calling thread's workspace,
+ * valid until that thread's next build call (copy them out to keep them).
+ * Layout is the same as nlb_result (edge_index = [src | dst], shift xyz).
+ * Used by GNN pipelines that consume edge_index on the GPU (e.g. through
+ * DLPack / torch) and by bench.py's device-resident measurement. */
+typedef struct nlb_device_result {
+  int64_t n_edges;
+  int64_t* edge_index; /* device, 2*M int64 */
+  int32_t* shift;      /* device, 3*M int32 */
+} nlb_device_result;
+
+int nlb_build_device(const double* d_positions, int64_t n_atoms, double cutoff,
+                     const double* cell, const uint8_t* pbc, nlb_device_result* out);
+
+/* Device-to-device copy on `stream` (a cudaStream_t): lets callers move a
+ * device result into memory they own before the next build. */
+int nlb_copy_device(void* dst, const void* src, size_t bytes, void* stream);
+
+/* Stream for the calling thread's subsequent calls (a cudaStream_t); NULL
+ * restores the library's own non-blocking stream. */
+void nlb_set_stream(void* stream);
+
+/* Kernel launches issued by this library since load (all threads). */
+int64_t nlb_kernel_launches(void);
+
+/* Per-thread phase timing with CUDA events on the launching stream.
+ * enable != 0 starts (and resets) it.  nlb_profile_read fills ms[0..3] with
+ * the accumulated device time of: grid build, count pass, offset scan, emit
+ * pass, and returns the number of profiled calls. */
+void nlb_profile(int enable);
+int64_t nlb_profile_read(double* ms);
+
 /* Cell helpers behind the Python PyCell class (src/python_api.rs:15-99).
  * nlb_cell_check: 0 if H is invertible, NLB_ERR_VALUE ("Cell matrix is not
  * invertible", src/cell.rs:18-21) otherwise.

@@ -212,7 +212,53 @@ __global__ void __launch_bounds__(kSortThreads)
   }
 }
 
+constexpr int kBoundsThreads = 1024;
+
+__global__ void __launch_bounds__(kBoundsThreads)
+    k_bounds(const double* __restrict__ pos, int64_t n, double* __restrict__ out) {
+  __shared__ double red[6][kBoundsThreads / 32];
+  double lo[3] = {INFINITY, INFINITY, INFINITY};
+  double hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double v = pos[3 * i + a];
+      if (v < lo[a]) lo[a] = v;
+      if (v > hi[a]) hi[a] = v;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const double l2 = __shfl_xor_sync(0xffffffffu, lo[a], o);
+      const double h2 = __shfl_xor_sync(0xffffffffu, hi[a], o);
+      if (l2 < lo[a]) lo[a] = l2;
+      if (h2 > hi[a]) hi[a] = h2;
+    }
+    if (lane == 0) {
+      red[a][warp] = lo[a];
+      red[3 + a][warp] = hi[a];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double l = INFINITY, h = -INFINITY;
+    for (int w = 0; w < kBoundsThreads / 32; ++w) {
+      if (red[threadIdx.x][w] < l) l = red[threadIdx.x][w];
+      if (red[3 + threadIdx.x][w] > h) h = red[3 + threadIdx.x][w];
+    }
+    out[threadIdx.x] = l;
+    out[3 + threadIdx.x] = h;
+  }
+}
+
 }  // namespace
+
+void launch_bounds(const double* pos, int64_t n, double* out, cudaStream_t s) {
+  k_bounds<<<1, kBoundsThreads, 0, s>>>(pos, n, out);
+  note_launches(1);
+}
 
 void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const GridBuffers& b,
                        cudaStream_t s) {
@@ -225,6 +271,7 @@ void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const 
                                                        b.skey, b.sidx);
   k_binsort<<<(unsigned)g.total_bins, kSortThreads, 0, s>>>(
       g, pos, b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta);
+  note_launches(4);
 }
 
 }  // namespace nlb

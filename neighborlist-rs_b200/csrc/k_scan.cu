@@ -94,15 +94,11 @@ constexpr size_t kStageBytes = sizeof(int64_t) * kTile;
 
 template <class TIn>
 void scan_impl(const TIn* in, int64_t n, int64_t* out, int64_t* tmp, cudaStream_t s) {
-  static bool configured = false;  // benign race: the attribute is idempotent
-  if (!configured) {
-    cudaFuncSetAttribute(scan_tiles<TIn>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kStageBytes);
-    configured = true;
-  }
+  ensure_smem_attr((const void*)scan_tiles<TIn>, (int)kStageBytes);
   const int64_t tiles = (n + kTile - 1) / kTile;
   if (tiles <= 1) {
     scan_tiles<TIn><<<1, kThreads, kStageBytes, s>>>(in, n, out, nullptr);
+    note_launches(1);
     return;
   }
   // tmp layout: [tile totals (tiles)] [scanned totals (tiles + 1)] [scratch...]
@@ -111,6 +107,7 @@ void scan_impl(const TIn* in, int64_t n, int64_t* out, int64_t* tmp, cudaStream_
   scan_tiles<TIn><<<(unsigned)tiles, kThreads, kStageBytes, s>>>(in, n, out, totals);
   scan_impl<int64_t>(totals, tiles, bases, tmp + 2 * tiles + 1, s);
   add_tile_bases<<<(unsigned)tiles, kThreads, 0, s>>>(out, n, bases);
+  note_launches(2);
 }
 
 }  // namespace

@@ -271,21 +271,25 @@ inline unsigned blocks_for(int64_t n) {
 void launch_grid_count(const GridParams& g, const GridBuffers& b, int64_t n,
                        const CutoffSet& cs, uint32_t* counts, cudaStream_t s) {
   k_grid_count<<<blocks_for(n), kWarpsPerBlock * 32, 0, s>>>(g, b, n, cs, counts);
+  note_launches(1);
 }
 
 void launch_grid_emit(const GridParams& g, const GridBuffers& b, int64_t n, const CutoffSet& cs,
                       const int64_t* offs, const EmitTargets& t, cudaStream_t s) {
   k_grid_emit<<<blocks_for(n), kWarpsPerBlock * 32, 0, s>>>(g, b, n, cs, offs, t);
+  note_launches(1);
 }
 
 void launch_brute_count(const BruteParams& bp, const double* pos, int64_t n, const CutoffSet& cs,
                         uint32_t* counts, cudaStream_t s) {
   k_brute_count<<<blocks_for(n), kWarpsPerBlock * 32, 0, s>>>(bp, pos, n, cs, counts);
+  note_launches(1);
 }
 
 void launch_brute_emit(const BruteParams& bp, const double* pos, int64_t n, const CutoffSet& cs,
                        const int64_t* offs, const EmitTargets& t, cudaStream_t s) {
   k_brute_emit<<<blocks_for(n), kWarpsPerBlock * 32, 0, s>>>(bp, pos, n, cs, offs, t);
+  note_launches(1);
 }
 
 }  // namespace nlb

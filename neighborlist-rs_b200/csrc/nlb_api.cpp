@@ -44,6 +44,12 @@ std::atomic<uint64_t> g_bf_threshold{1000};   // src/config.rs DEFAULT_BRUTE_FOR
 std::atomic<uint64_t> g_par_threshold{300};   // DEFAULT_PARALLEL_THRESHOLD
 std::atomic<uint64_t> g_stack_threshold{1000};  // DEFAULT_STACK_THRESHOLD
 
+std::atomic<int64_t> g_launches{0};
+void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+thread_local cudaStream_t tl_user_stream = nullptr;
+thread_local bool tl_profile = false;
+
 // ------------------------------------------------------------------ pinned pool
 
 namespace {
@@ -129,20 +135,44 @@ Status get_ctx(Ctx** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice (is a CUDA device present?)");
+  Ctx* c = nullptr;
   auto it = ctxs.find(dev);
   if (it != ctxs.end()) {
-    *out = it->second;
-    return Status{NLB_OK};
+    c = it->second;
+  } else {
+    c = new Ctx();  // lives for the thread's lifetime; never freed at exit
+    c->device = dev;
+    e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    e = cudaHostAlloc((void**)&c->h_small, sizeof(int64_t) * kSmallHost, cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+    for (int i = 0; i < 6; ++i) cudaEventCreate(&c->ev[i]);
+    ctxs[dev] = c;
   }
-  Ctx* c = new Ctx();  // lives for the thread's lifetime; never freed at exit
-  c->device = dev;
-  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
-  e = cudaHostAlloc((void**)&c->h_small, sizeof(int64_t) * kSmallHost, cudaHostAllocDefault);
-  if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
-  ctxs[dev] = c;
+  c->stream = tl_user_stream ? tl_user_stream : c->own_stream;
+  if (tl_profile != c->prof) {
+    c->prof = tl_profile;
+    c->prof_pending_count = c->prof_pending_emit = false;
+  }
   *out = c;
   return Status{NLB_OK};
+}
+
+// Accumulates the phase times of completed (synchronized) profiled work.
+void Ctx::harvest() {
+  float ms = 0.f;
+  if (prof_pending_count) {
+    if (cudaEventElapsedTime(&ms, ev[0], ev[1]) == cudaSuccess) prof_ms[0] += ms;
+    if (cudaEventElapsedTime(&ms, ev[1], ev[2]) == cudaSuccess) prof_ms[1] += ms;
+    if (cudaEventElapsedTime(&ms, ev[2], ev[3]) == cudaSuccess) prof_ms[2] += ms;
+    prof_pending_count = false;
+  }
+  if (prof_pending_emit) {
+    if (cudaEventElapsedTime(&ms, ev[4], ev[5]) == cudaSuccess) prof_ms[3] += ms;
+    prof_pending_emit = false;
+    prof_calls += 1;
+  }
+  cudaGetLastError();
 }
 
 void ensure_smem_attr(const void* func, int bytes) {
@@ -173,6 +203,7 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
                                           (int64_t)k * (n + 1), sp.grid.total_bins)));
   if (!sp.counts || !sp.offs || !scan_tmp) return fail(NLB_ERR_NOMEM, "device allocation failed");
 
+  c.mark(0);
   if (sp.method == Method::kCellList) {
     GridBuffers& b = sp.gb;
     const int64_t nb = sp.grid.total_bins;
@@ -198,6 +229,7 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
     cudaMemsetAsync(b.bin_fill, 0, sizeof(int32_t) * nb, s);
     launch_grid_build(sp.grid, d_pos, n, b, s);
   }
+  c.mark(1);
   for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
     CutoffSet cs = sp.pass(g0);
     uint32_t* rows = sp.counts + (size_t)g0 * (n + 1);
@@ -206,7 +238,9 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
     else
       launch_brute_count(sp.brute, d_pos, n, cs, rows, s);
   }
+  c.mark(2);
   exclusive_scan_u32(sp.counts, (int64_t)k * (n + 1), sp.offs, scan_tmp, s);
+  c.mark(3);
   // Row starts offs[q * (n + 1)], q = 0..k, in one strided copy.
   if (k + 1 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
   cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), sp.offs, sizeof(int64_t) * (n + 1),
@@ -214,6 +248,11 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy2DAsync");
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "count pass");
+  if (c.prof) {
+    c.harvest();  // a previous emit on this stream is complete too
+    c.prof_pending_count = true;
+    c.harvest();
+  }
   sp.m.resize(k);
   for (int32_t q = 0; q < k; ++q) sp.m[q] = c.h_small[q + 1] - c.h_small[q];
   return Status{NLB_OK};
@@ -223,6 +262,7 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
 Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& L,
                    const int64_t* base, int64_t index_offset) {
   const int32_t k = (int32_t)sp.rc_sq.size();
+  c.mark(4);
   for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
     CutoffSet cs = sp.pass(g0);
     EmitTargets t;
@@ -240,6 +280,8 @@ Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& 
     else
       launch_brute_emit(sp.brute, d_pos, sp.n, cs, offs, t, c.stream);
   }
+  c.mark(5);
+  if (c.prof) c.prof_pending_emit = true;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "emit launch");
   return Status{NLB_OK};
@@ -260,7 +302,7 @@ CutoffSet SystemPlan::pass(int32_t g0) const {
 // Validates and plans one system (cell or auto-box, dispatch, grid).
 Status plan_system(const double* pos_host, int64_t n, const double* cell9, const bool pbc[3],
                    const std::vector<double>& cutoffs, bool disjoint, bool multi,
-                   SystemPlan& sp) {
+                   SystemPlan& sp, const double* bounds6) {
   sp.n = n;
   sp.disjoint = disjoint;
   const int32_t k = (int32_t)cutoffs.size();
@@ -269,6 +311,9 @@ Status plan_system(const double* pos_host, int64_t n, const double* cell9, const
   std::string err;
   if (cell9) {
     if (!make_cell(cell9, pbc, sp.cell, err)) return fail(NLB_ERR_VALUE, err);
+  } else if (bounds6) {
+    if (!auto_box_from_bounds(bounds6, bounds6 + 3, rc_max, sp.cell, err))
+      return fail(NLB_ERR_VALUE, err);
   } else {
     if (!auto_box(pos_host, n, rc_max, sp.cell, err)) return fail(NLB_ERR_VALUE, err);
   }
@@ -368,6 +413,7 @@ Status download_results(Ctx& c, const std::vector<int64_t>& m, const DevLists& L
   }
   cudaError_t e = cudaStreamSynchronize(c.stream);
   if (e != cudaSuccess) return cuda_fail(e, "emit pass");
+  if (c.prof) c.harvest();
   return Status{NLB_OK};
 }
 
@@ -422,6 +468,53 @@ Status run_single(const double* pos, int64_t n, const double* cell9, const uint8
     for (int32_t q = 0; q < k; ++q) nlb_result_free(&outs[q]);
   }
   return st;
+}
+
+// One system, one cutoff, device in / device out (nlb_build_device).
+Status run_single_device(const double* d_pos, int64_t n, const double* cell9, const uint8_t* pbc,
+                         double cutoff, nlb_device_result* out) {
+  out->n_edges = 0;
+  out->edge_index = nullptr;
+  out->shift = nullptr;
+  if (!cutoffs_valid(&cutoff, 1)) return fail(NLB_ERR_VALUE, "Cutoff must be positive and finite");
+  if (n < 0) return fail(NLB_ERR_VALUE, "Positions must be (N, 3)");
+  if (n == 0) return Status{NLB_OK};
+  if (!d_pos) return fail(NLB_ERR_VALUE, "positions is NULL");
+  Ctx* c = nullptr;
+  Status st = get_ctx(&c);
+  if (!st.ok()) return st;
+  double bounds[6];
+  const double* bptr = nullptr;
+  if (!cell9) {
+    double* d_b = static_cast<double*>(c->raw(kSlotBatch0 + 31, sizeof(double) * 6));
+    if (!d_b) return fail(NLB_ERR_NOMEM, "device allocation failed");
+    launch_bounds(d_pos, n, d_b, c->stream);
+    cudaError_t e = cudaMemcpyAsync(bounds, d_b, sizeof(bounds), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "bounds");
+    bptr = bounds;
+  }
+  const bool pb[3] = {pbc ? pbc[0] != 0 : true, pbc ? pbc[1] != 0 : true,
+                      pbc ? pbc[2] != 0 : true};
+  SystemPlan sp;
+  std::vector<double> cs(1, cutoff);
+  st = plan_system(nullptr, n, cell9, pb, cs, false, false, sp, bptr);
+  if (!st.ok()) return st;
+  st = count_system(*c, sp, d_pos);
+  if (!st.ok()) return st;
+  DevLists L;
+  st = device_outputs(*c, sp.m, L);
+  if (!st.ok()) return st;
+  const int64_t zero = 0;
+  st = emit_system(*c, sp, d_pos, L, &zero, 0);
+  if (!st.ok()) return st;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "emit pass");
+  if (c->prof) c->harvest();
+  out->n_edges = sp.m[0];
+  out->edge_index = L.src[0];
+  out->shift = L.sh[0];
+  return Status{NLB_OK};
 }
 
 }  // namespace nlb
@@ -479,6 +572,42 @@ void nlb_result_free(nlb_result* r) {
 }
 
 void nlb_host_free(void* p) { pinned_release(p); }
+
+int nlb_build_device(const double* d_positions, int64_t n_atoms, double cutoff,
+                     const double* cell, const uint8_t* pbc, nlb_device_result* out) {
+  if (!out) return fail(NLB_ERR_VALUE, "out is NULL").code;
+  return run_single_device(d_positions, n_atoms, cell, pbc, cutoff, out).code;
+}
+
+int nlb_copy_device(void* dst, const void* src, size_t bytes, void* stream) {
+  if (bytes == 0) return NLB_OK;
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice,
+                                  static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(e, "nlb_copy_device").code;
+  return NLB_OK;
+}
+
+void nlb_set_stream(void* stream) { tl_user_stream = static_cast<cudaStream_t>(stream); }
+
+int64_t nlb_kernel_launches(void) { return g_launches.load(); }
+
+void nlb_profile(int enable) {
+  tl_profile = enable != 0;
+  Ctx* c = nullptr;
+  if (get_ctx(&c).ok()) {
+    c->prof_ms[0] = c->prof_ms[1] = c->prof_ms[2] = c->prof_ms[3] = 0.0;
+    c->prof_calls = 0;
+    c->prof_pending_count = c->prof_pending_emit = false;
+  }
+}
+
+int64_t nlb_profile_read(double* ms) {
+  Ctx* c = nullptr;
+  if (!get_ctx(&c).ok()) return -1;
+  if (ms)
+    for (int i = 0; i < 4; ++i) ms[i] = c->prof_ms[i];
+  return c->prof_calls;
+}
 
 int nlb_cell_check(const double* cell) {
   if (!cell) return fail(NLB_ERR_VALUE, "cell is NULL").code;

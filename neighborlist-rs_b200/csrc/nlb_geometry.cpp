@@ -89,6 +89,11 @@ bool auto_box(const double* pos, int64_t n, double rc_max, HostCell& c, std::str
       if (v < lo[a]) lo[a] = v;
       if (v > hi[a]) hi[a] = v;
     }
+  return auto_box_from_bounds(lo, hi, rc_max, c, err);
+}
+
+bool auto_box_from_bounds(const double* lo, const double* hi, double rc_max, HostCell& c,
+                          std::string& err) {
   const double margin = rc_max + 1.0;
   double h9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int a = 0; a < 3; ++a) h9[4 * a] = (hi[a] - lo[a]) + 2.0 * margin;

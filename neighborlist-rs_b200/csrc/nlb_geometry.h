@@ -27,6 +27,9 @@ bool make_cell(const double* h9, const bool pbc[3], HostCell& c, std::string& er
 
 // Orthorhombic box diag(span + 2 (rc + 1)), origin 0, no periodicity.
 bool auto_box(const double* pos, int64_t n, double rc_max, HostCell& c, std::string& err);
+// Same, from precomputed per-axis bounds lo[3], hi[3].
+bool auto_box_from_bounds(const double* lo, const double* hi, double rc_max, HostCell& c,
+                          std::string& err);
 
 void perpendicular_widths(const HostCell& c, double w[3]);
 

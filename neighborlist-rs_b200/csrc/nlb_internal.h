@@ -56,9 +56,22 @@ struct Ctx {
     size_t cap = 0;
   };
   int device = 0;
-  cudaStream_t stream = nullptr;
-  int64_t* h_small = nullptr;  // pinned scratch for small device->host reads
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;  // active stream: the caller's (nlb_set_stream) or own_stream
+  int64_t* h_small = nullptr;     // pinned scratch for small device->host reads
   Buf bufs[kSlotCount];
+  // Phase timing (nlb_profile): events ev[0..3] bracket build / count / scan,
+  // ev[4..5] the emit pass; harvested after the stream is synchronized.
+  bool prof = false;
+  bool prof_pending_count = false;
+  bool prof_pending_emit = false;
+  cudaEvent_t ev[6] = {};
+  double prof_ms[4] = {0, 0, 0, 0};
+  int64_t prof_calls = 0;
+  void mark(int i) {
+    if (prof) cudaEventRecord(ev[i], stream);
+  }
+  void harvest();
   // Returns a device buffer of at least `bytes` for `slot` (contents are not
   // preserved on growth), or nullptr if the allocation failed.
   void* raw(int slot, size_t bytes);
@@ -99,9 +112,11 @@ struct DevLists {
   std::vector<int32_t*> sh;
 };
 
+// bounds6 (optional): per-axis min[3], max[3] of the positions for the
+// auto-box when the positions are not on the host.
 Status plan_system(const double* pos_host, int64_t n, const double* cell9, const bool pbc[3],
                    const std::vector<double>& cutoffs, bool disjoint, bool multi,
-                   SystemPlan& sp);
+                   SystemPlan& sp, const double* bounds6 = nullptr);
 Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos);
 Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& L,
                    const int64_t* base, int64_t index_offset);

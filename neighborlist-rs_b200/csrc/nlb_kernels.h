@@ -78,4 +78,12 @@ void launch_brute_emit(const BruteParams& bp, const double* pos, int64_t n, cons
 // Sets the dynamic shared-memory limit of a kernel once per device.
 void ensure_smem_attr(const void* func, int bytes);
 
+// Counts kernel launches issued by this library (reported by nlb_kernel_launches).
+void note_launches(int n);
+
+// ---- k_grid.cu : per-axis min / max of device positions (auto-box bounds)
+// out[0..2] = min, out[3..5] = max (NaN coordinates are ignored, like the
+// reference's `<` / `>` scan starting from +/-inf).
+void launch_bounds(const double* pos, int64_t n, double* out, cudaStream_t s);
+
 }  // namespace nlb

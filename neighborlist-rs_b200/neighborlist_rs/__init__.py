@@ -393,3 +393,97 @@ def set_stack_threshold(val) -> None:
 
 def version() -> str:
     return _lib.nlb_version().decode()
+
+
+# ---------------------------------------------------------------- device-resident path
+
+class _DevResult(ctypes.Structure):
+    _fields_ = [("n_edges", ctypes.c_int64),
+                ("edge_index", ctypes.c_void_p),
+                ("shift", ctypes.c_void_p)]
+
+
+_lib.nlb_build_device.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, _dp, _u8p,
+                                  ctypes.POINTER(_DevResult)]
+_lib.nlb_set_stream.argtypes = [ctypes.c_void_p]
+_lib.nlb_kernel_launches.restype = ctypes.c_int64
+_lib.nlb_profile.argtypes = [ctypes.c_int]
+_lib.nlb_profile_read.argtypes = [_dp]
+_lib.nlb_profile_read.restype = ctypes.c_int64
+
+
+def set_stream(stream_handle: int | None) -> None:
+    """Launch the calling thread's subsequent builds on this cudaStream_t
+    (e.g. ``torch.cuda.current_stream().cuda_stream``); None = library stream."""
+    _lib.nlb_set_stream(ctypes.c_void_p(stream_handle) if stream_handle else None)
+
+
+def kernel_launches() -> int:
+    return int(_lib.nlb_kernel_launches())
+
+
+def profile(enable: bool) -> None:
+    _lib.nlb_profile(int(bool(enable)))
+
+
+def profile_read():
+    """(calls, {build, count, scan, emit} ms accumulated with CUDA events)."""
+    ms = np.zeros(4, np.float64)
+    calls = int(_lib.nlb_profile_read(ms.ctypes.data_as(_dp)))
+    return calls, dict(zip(("build", "count", "scan", "emit"), ms.tolist()))
+
+
+def build_device_raw(cell, positions_ptr: int, n_atoms: int, cutoff: float):
+    """Device-resident build: positions_ptr is a device pointer to n x 3
+    float64.  Returns (n_edges, edge_index_ptr, shift_ptr): device pointers
+    into the calling thread's workspace, valid until its next build."""
+    c = _check_cutoff(cutoff)
+    h, pb = _cell_args(cell)
+    r = _DevResult()
+    _check(_lib.nlb_build_device(ctypes.c_void_p(positions_ptr), int(n_atoms), c, h, pb,
+                                 ctypes.byref(r)))
+    return int(r.n_edges), r.edge_index, r.shift
+
+
+def build_neighborlists_torch(cell, positions, cutoff):
+    """GPU-resident variant of build_neighborlists for torch pipelines:
+    ``positions`` is a CUDA float64 tensor (N, 3); returns
+    {"edge_index": int64 (2, M), "shift": int32 (M, 3)} as CUDA tensors on the
+    same device, produced on the current torch stream (no host round trip
+    for the edge arrays)."""
+    import torch
+
+    if not (isinstance(positions, torch.Tensor) and positions.is_cuda
+            and positions.dtype == torch.float64 and positions.dim() == 2):
+        raise TypeError("positions must be a CUDA float64 tensor of shape (N, 3)")
+    if positions.shape[1] != 3:
+        raise ValueError("Positions must be (N, 3)")
+    pos = positions.contiguous()
+    dev = pos.device
+    n = pos.shape[0]
+    if n == 0:
+        _check_cutoff(cutoff)
+        return {"edge_index": torch.zeros((2, 0), dtype=torch.int64, device=dev),
+                "shift": torch.zeros((0, 3), dtype=torch.int32, device=dev)}
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev)
+        set_stream(stream.cuda_stream)
+        try:
+            m, ei_ptr, sh_ptr = build_device_raw(cell, pos.data_ptr(), n, cutoff)
+            ei = torch.empty((2, m), dtype=torch.int64, device=dev)
+            sh = torch.empty((m, 3), dtype=torch.int32, device=dev)
+            if m:
+                _cudart_copy(ei.data_ptr(), ei_ptr, 16 * m, stream.cuda_stream)
+                _cudart_copy(sh.data_ptr(), sh_ptr, 12 * m, stream.cuda_stream)
+        finally:
+            set_stream(None)
+    return {"edge_index": ei, "shift": sh}
+
+
+_lib.nlb_copy_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                 ctypes.c_void_p]
+
+
+def _cudart_copy(dst, src, nbytes, stream):
+    _check(_lib.nlb_copy_device(ctypes.c_void_p(dst), ctypes.c_void_p(src), nbytes,
+                                ctypes.c_void_p(stream)))
