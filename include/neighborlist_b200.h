@@ -130,6 +130,28 @@ int64_t nlb_kernel_launches(void);
 void nlb_profile(int enable);
 int64_t nlb_profile_read(double* ms);
 
+/* ---- Build without allocating (no counterpart in the reference). ----
+ * For callers that must not allocate GPU memory when they ask for a list:
+ * processes whose HBM is held by a framework's caching allocator, code that
+ * cannot afford cudaFree's device-wide synchronisation, and loops that only
+ * allocate at start-up.  Single system, one cutoff, same edges in the same
+ * order as nlb_build / nlb_build_device.  The caller passes device positions
+ * (n x 3 float64) and device outputs: d_edge_index with room for
+ * 2 x max_edges int64 (sources in [0, M), destinations in
+ * [max_edges, max_edges + M)) and d_shift with room for max_edges x 3 int32;
+ * *n_edges (host) receives M.  All scratch lives in one fixed __device__
+ * array inside the library (about 1.8 MB per device, held until exit), so
+ * systems are limited to 16384 atoms and 16384 cell-list bins; larger inputs
+ * and M > max_edges are rejected with NLB_ERR_VALUE (outputs untouched when
+ * M > max_edges; *n_edges still reports M).  The first call on each device
+ * looks up the array's device address (make it before any stream capture).
+ * Calls share the array: calls that overlap on one device race and must be
+ * serialised.  Runs on `stream` (a cudaStream_t, NULL = legacy default) and
+ * returns after the results are complete. */
+int nlb_build_noalloc(const double* d_positions, int64_t n_atoms, double cutoff,
+                      const double* cell, const uint8_t* pbc, int64_t* d_edge_index,
+                      int32_t* d_shift, int64_t max_edges, int64_t* n_edges, void* stream);
+
 /* Cell helpers behind the Python PyCell class (src/python_api.rs:15-99).
  * nlb_cell_check: 0 if H is invertible, NLB_ERR_VALUE ("Cell matrix is not
  * invertible", src/cell.rs:18-21) otherwise.
