@@ -1,0 +1,539 @@
+// k_batch.cu -- many small systems per launch (src/batch.rs:10-290).
+//
+//   k_plan        one warp per system: auto-box bounds (when the system has no
+//                 cell), H^-1, perpendicular widths, mic_safe and the
+//                 brute-force / cell-list dispatch, and the grid (bins,
+//                 stencil half-widths, prune geometry) -- the same f64
+//                 expressions, in the same order, as the host planner
+//                 (nlb_geometry.cpp) and the reference (src/single.rs:8-164,
+//                 src/search.rs:119-246).
+//   k_batch_count / k_batch_emit
+//                 persistent CTAs pull systems from a work queue (largest
+//                 first).  A CTA keeps its whole system in shared memory:
+//                 for the cell list it sorts the atoms by (bin Morton code,
+//                 atom Morton key, index) -- bin code order is bin rank
+//                 order, so no rank table is needed -- and finds a stencil
+//                 cell's atoms by binary search on the sorted codes.  Warps
+//                 then walk one atom each, exactly like the single-system
+//                 kernels, and count or emit through the shared sinks.
+// Per-atom counts of all systems form one flat row per cutoff; one exclusive
+// scan gives every system's global edge offsets, so the emit pass writes the
+// concatenated, exact-sized output (systems in input order) directly.
+#include "k_traverse.cuh"
+
+namespace nlb {
+
+namespace {
+
+constexpr int kBatchThreads = 256;
+constexpr int kBatchWarps = kBatchThreads / 32;
+
+__device__ __forceinline__ double dfmin(double a, double b) {
+  if (a != a) return b;
+  if (b != b) return a;
+  return a < b ? a : b;
+}
+__device__ __forceinline__ double dfmax(double a, double b) {
+  if (a != a) return b;
+  if (b != b) return a;
+  return a > b ? a : b;
+}
+
+// Device mirror of make_cell (nalgebra 3x3 inverse).  Returns false if det == 0.
+__device__ bool dev_make_cell(const double* h, double* hinv) {
+  const double m11 = h[0], m12 = h[1], m13 = h[2];
+  const double m21 = h[3], m22 = h[4], m23 = h[5];
+  const double m31 = h[6], m32 = h[7], m33 = h[8];
+  const double ca = dsub(dmul(m22, m33), dmul(m32, m23));
+  const double cb = dsub(dmul(m21, m33), dmul(m31, m23));
+  const double cc = dsub(dmul(m21, m32), dmul(m31, m22));
+  const double det = dadd(dsub(dmul(m11, ca), dmul(m12, cb)), dmul(m13, cc));
+  if (det == 0.0) return false;
+  hinv[0] = __ddiv_rn(ca, det);
+  hinv[1] = __ddiv_rn(dsub(dmul(m13, m32), dmul(m33, m12)), det);
+  hinv[2] = __ddiv_rn(dsub(dmul(m12, m23), dmul(m22, m13)), det);
+  hinv[3] = __ddiv_rn(-cb, det);
+  hinv[4] = __ddiv_rn(dsub(dmul(m11, m33), dmul(m31, m13)), det);
+  hinv[5] = __ddiv_rn(dsub(dmul(m13, m21), dmul(m23, m11)), det);
+  hinv[6] = __ddiv_rn(cc, det);
+  hinv[7] = __ddiv_rn(dsub(dmul(m12, m31), dmul(m32, m11)), det);
+  hinv[8] = __ddiv_rn(dsub(dmul(m11, m22), dmul(m21, m12)), det);
+  return true;
+}
+
+__device__ void dev_widths(const double* hinv, double* w) {
+  for (int r = 0; r < 3; ++r)
+    w[r] = __ddiv_rn(1.0, __dsqrt_rn(norm2(hinv[3 * r], hinv[3 * r + 1], hinv[3 * r + 2])));
+}
+
+__device__ __forceinline__ void mv_plain(const double* m, double v0, double v1, double v2,
+                                         double* out) {
+  matvec(m, v0, v1, v2, out);
+}
+
+// Device mirror of plan_grid (host) for cutoff rc.
+__device__ void dev_plan_grid(const double* w, double rc, GridParams& g) {
+  int64_t total = 1;
+  for (int a = 0; a < 3; ++a) {
+    uint64_t b = sat_u64(floor(__ddiv_rn(w[a], rc)));
+    if (b < 1) b = 1;
+    if (b > 2147483647ull) b = 2147483647ull;
+    g.nb[a] = (int32_t)b;
+    total *= (int64_t)g.nb[a];
+    if (total > ((int64_t)1 << 40)) total = ((int64_t)1 << 40);
+  }
+  g.total_bins = total;
+  for (int a = 0; a < 3; ++a) g.ns[a] = sat_i32(ceil(__ddiv_rn(dmul(rc, (double)g.nb[a]), w[a])));
+  double vb[3][3];
+  mv_plain(g.h, __ddiv_rn(1.0, (double)g.nb[0]), 0.0, 0.0, vb[0]);
+  mv_plain(g.h, 0.0, __ddiv_rn(1.0, (double)g.nb[1]), 0.0, vb[1]);
+  mv_plain(g.h, 0.0, 0.0, __ddiv_rn(1.0, (double)g.nb[2]), vb[2]);
+  mv_plain(g.h, __ddiv_rn(0.5, (double)g.nb[0]), __ddiv_rn(0.5, (double)g.nb[1]),
+           __ddiv_rn(0.5, (double)g.nb[2]), g.origin);
+  for (int a = 0; a < 3; ++a)
+    for (int k = 0; k < 3; ++k) g.basis[a][k] = vb[a][k];
+  double d[4], t[3];
+  for (int k = 0; k < 3; ++k) t[k] = dadd(dadd(vb[0][k], vb[1][k]), vb[2][k]);
+  d[0] = norm2(t[0], t[1], t[2]);
+  for (int k = 0; k < 3; ++k) t[k] = dsub(dadd(vb[0][k], vb[1][k]), vb[2][k]);
+  d[1] = norm2(t[0], t[1], t[2]);
+  for (int k = 0; k < 3; ++k) t[k] = dadd(dsub(vb[0][k], vb[1][k]), vb[2][k]);
+  d[2] = norm2(t[0], t[1], t[2]);
+  for (int k = 0; k < 3; ++k) t[k] = dsub(dsub(vb[0][k], vb[1][k]), vb[2][k]);
+  d[3] = norm2(t[0], t[1], t[2]);
+  const double mx = dfmax(dfmax(dfmax(d[0], d[1]), d[2]), d[3]);
+  const double radius = dmul(0.5, __dsqrt_rn(mx));
+  const double pl = dadd(__dsqrt_rn(dmul(rc, rc)), radius);
+  g.prune_sq = dmul(pl, pl);
+}
+
+__global__ void k_plan(const double* __restrict__ pos, const int64_t* __restrict__ starts,
+                       int32_t s0, int32_t s1, const double* __restrict__ cells,
+                       const uint8_t* __restrict__ pbcs, const uint8_t* __restrict__ has_cell,
+                       double rc_max, uint64_t bf_threshold, int multi, int64_t run_start,
+                       SysPlan* __restrict__ plans, int32_t* __restrict__ error_flag) {
+  const int lane = threadIdx.x & 31;
+  const int32_t s = s0 + blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (s >= s1) return;
+  const int64_t b = starts[s], e = starts[s + 1];
+  const bool own_cell = cells && has_cell && has_cell[s];
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  if (!own_cell) {
+    for (int64_t i = b + lane; i < e; i += 32)
+      for (int a = 0; a < 3; ++a) {
+        const double v = pos[3 * i + a];
+        if (v < lo[a]) lo[a] = v;
+        if (v > hi[a]) hi[a] = v;
+      }
+    for (int a = 0; a < 3; ++a)
+      for (int o = 16; o > 0; o >>= 1) {
+        const double l2 = __shfl_xor_sync(0xffffffffu, lo[a], o);
+        const double h2 = __shfl_xor_sync(0xffffffffu, hi[a], o);
+        if (l2 < lo[a]) lo[a] = l2;
+        if (h2 > hi[a]) hi[a] = h2;
+      }
+  }
+  if (lane != 0) return;
+  SysPlan P;
+  P.start = b;
+  P.n = (int32_t)(e - b);
+  P.slot = b - run_start;
+  GridParams& g = P.g;
+  for (int i = 0; i < 9; ++i) g.h[i] = 0.0;
+  if (own_cell) {
+    for (int i = 0; i < 9; ++i) g.h[i] = cells[9 * s + i];
+    for (int a = 0; a < 3; ++a) P.pbc[a] = pbcs ? (pbcs[3 * s + a] != 0) : 1;
+  } else {
+    const double margin = dadd(rc_max, 1.0);
+    for (int a = 0; a < 3; ++a) g.h[4 * a] = dadd(dsub(hi[a], lo[a]), dmul(2.0, margin));
+    P.pbc[0] = P.pbc[1] = P.pbc[2] = 0;
+  }
+  if (!dev_make_cell(g.h, g.hinv)) {
+    P.method = -1;
+    atomicExch(error_flag, 1);
+    plans[s - s0] = P;
+    return;
+  }
+  double w[3];
+  dev_widths(g.hinv, w);
+  const double min_w = dfmin(dfmin(w[0], w[1]), w[2]);
+  const bool mic_safe = dmul(rc_max, 2.0) < min_w;
+  if ((uint64_t)P.n < bf_threshold && mic_safe) {
+    const bool isolated = !P.pbc[0] && !P.pbc[1] && !P.pbc[2];
+    P.method = (isolated && !multi) ? 0 : 1;
+    g.total_bins = 0;
+  } else {
+    P.method = 2;
+    dev_plan_grid(w, rc_max, g);
+    for (int a = 0; a < 3; ++a)
+      if (g.ns[a] < 0 || g.ns[a] > (1 << 20)) atomicExch(error_flag, 2);
+  }
+  plans[s - s0] = P;
+}
+
+// ------------------------------------------------------------------ shared memory
+
+struct SmemView {
+  uint64_t* bcode;  // [cap] sort key 1 (bin Morton code), sorted
+  uint64_t* key;    // [cap] sort key 2 (atom Morton key)
+  int32_t* idx;     // [cap] sort key 3 (local atom index)
+  double* px;       // [cap] wrapped (cell list) or raw (brute) positions
+  double* py;
+  double* pz;
+  SlotMeta* meta;   // [cap]
+};
+
+__device__ __forceinline__ SmemView smem_view(unsigned char* base, int cap) {
+  SmemView v;
+  v.bcode = reinterpret_cast<uint64_t*>(base);
+  v.key = v.bcode + cap;
+  v.px = reinterpret_cast<double*>(v.key + cap);
+  v.py = v.px + cap;
+  v.pz = v.py + cap;
+  v.meta = reinterpret_cast<SlotMeta*>(v.pz + cap);
+  v.idx = reinterpret_cast<int32_t*>(v.meta + cap);
+  return v;
+}
+
+__device__ __forceinline__ bool triple_less(uint64_t a0, uint64_t a1, int32_t a2, uint64_t b0,
+                                            uint64_t b1, int32_t b2) {
+  if (a0 != b0) return a0 < b0;
+  if (a1 != b1) return a1 < b1;
+  return a2 < b2;
+}
+
+__device__ void sort_triples(const SmemView& v, int n) {
+  int p = 1;
+  while (p < n) p <<= 1;
+  for (int i = n + threadIdx.x; i < p; i += blockDim.x) {
+    v.bcode[i] = ~0ull;
+    v.key[i] = ~0ull;
+    v.idx[i] = 0x7fffffff;
+  }
+  __syncthreads();
+  for (int size = 2; size <= p; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < p; i += blockDim.x) {
+        const int j = i ^ stride;
+        if (j > i) {
+          const bool up = (i & size) == 0;
+          const bool gt = triple_less(v.bcode[j], v.key[j], v.idx[j], v.bcode[i], v.key[i], v.idx[i]);
+          if (gt == up) {
+            uint64_t t0 = v.bcode[i];
+            v.bcode[i] = v.bcode[j];
+            v.bcode[j] = t0;
+            uint64_t t1 = v.key[i];
+            v.key[i] = v.key[j];
+            v.key[j] = t1;
+            int32_t t2 = v.idx[i];
+            v.idx[i] = v.idx[j];
+            v.idx[j] = t2;
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+__device__ __forceinline__ uint64_t bin_code(int32_t bx, int32_t by, int32_t bz) {
+  return spread_bits3((uint64_t)bx) | (spread_bits3((uint64_t)by) << 1) |
+         (spread_bits3((uint64_t)bz) << 2);
+}
+
+// Loads one system into shared memory.  Cell list: sorted SoA in canonical
+// order (bin rank, Morton key, index).  Brute force: raw positions.
+__device__ void load_system(const SysPlan& P, const double* __restrict__ pos, const SmemView& v) {
+  const int n = P.n;
+  const double* sp = pos + 3 * P.start;
+  if (P.method != 2) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      v.px[i] = sp[3 * i];
+      v.py[i] = sp[3 * i + 1];
+      v.pz[i] = sp[3 * i + 2];
+    }
+    __syncthreads();
+    return;
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const AtomWrap w = wrap_atom(P.g, sp[3 * i], sp[3 * i + 1], sp[3 * i + 2]);
+    v.bcode[i] = bin_code(w.bin[0], w.bin[1], w.bin[2]);
+    v.key[i] = w.key;
+    v.idx[i] = i;
+  }
+  __syncthreads();
+  sort_triples(v, n);
+  for (int p = threadIdx.x; p < n; p += blockDim.x) {
+    const int i = v.idx[p];
+    const AtomWrap w = wrap_atom(P.g, sp[3 * i], sp[3 * i + 1], sp[3 * i + 2]);
+    v.px[p] = w.wx;
+    v.py[p] = w.wy;
+    v.pz[p] = w.wz;
+    SlotMeta m;
+    m.sx = w.s[0];
+    m.sy = w.s[1];
+    m.sz = w.s[2];
+    m.orig = i;
+    v.meta[p] = m;
+  }
+  __syncthreads();
+}
+
+// First index in [0, n) whose code is >= c.
+__device__ __forceinline__ int lower_bound_code(const uint64_t* codes, int n, uint64_t c) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (codes[mid] < c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+template <class Sink>
+__device__ __forceinline__ void visit_smem_grid_atom(const SysPlan& P, const SmemView& v, int p,
+                                                     double max_sq, Sink& sink) {
+  const GridParams& g = P.g;
+  const int lane = threadIdx.x & 31;
+  const int n = P.n;
+  const double pix = v.px[p], piy = v.py[p], piz = v.pz[p];
+  const SlotMeta mi = v.meta[p];
+  double fi[3];
+  matvec(g.hinv, pix, piy, piz, fi);
+  int32_t home[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int32_t hb = sat_i32(dmul(fi[a], (double)g.nb[a]));
+    home[a] = hb < g.nb[a] - 1 ? hb : g.nb[a] - 1;
+  }
+  const int32_t ny = 2 * g.ns[1] + 1, nz = 2 * g.ns[2] + 1;
+  const int64_t n_cells = (int64_t)(2 * g.ns[0] + 1) * ny * nz;
+  for (int64_t c0 = 0; c0 < n_cells; c0 += 32) {
+    const int64_t c = c0 + lane;
+    bool ok = c < n_cells;
+    int b0 = 0, b1 = 0;
+    double off[3] = {0.0, 0.0, 0.0};
+    int32_t sh[3] = {0, 0, 0};
+    if (ok) {
+      const int32_t ix = (int32_t)(c / ((int64_t)ny * nz));
+      const int32_t rem = (int32_t)(c - (int64_t)ix * ny * nz);
+      const int32_t iy = rem / nz, iz = rem - (rem / nz) * nz;
+      int32_t bin[3];
+      div_mod(home[0] + ix - g.ns[0], g.nb[0], bin[0], sh[0]);
+      div_mod(home[1] + iy - g.ns[1], g.nb[1], bin[1], sh[1]);
+      div_mod(home[2] + iz - g.ns[2], g.nb[2], bin[2], sh[2]);
+      double cs[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        off[k] = dadd(dadd(dmul(g.h[3 * k], (double)sh[0]), dmul(g.h[3 * k + 1], (double)sh[1])),
+                      dmul(g.h[3 * k + 2], (double)sh[2]));
+        double t = dadd(g.origin[k], dmul(g.basis[0][k], (double)bin[0]));
+        t = dadd(t, dmul(g.basis[1][k], (double)bin[1]));
+        t = dadd(t, dmul(g.basis[2][k], (double)bin[2]));
+        cs[k] = dadd(t, off[k]);
+      }
+      if (norm2(dsub(cs[0], pix), dsub(cs[1], piy), dsub(cs[2], piz)) > g.prune_sq) {
+        ok = false;
+      } else {
+        const uint64_t code = bin_code(bin[0], bin[1], bin[2]);
+        b0 = lower_bound_code(v.bcode, n, code);
+        b1 = code == ~0ull ? n : lower_bound_code(v.bcode, n, code + 1);
+        ok = b1 > b0;
+      }
+    }
+    unsigned cells = __ballot_sync(0xffffffffu, ok);
+    while (cells) {
+      const int src = __ffs(cells) - 1;
+      cells &= cells - 1;
+      const int j0 = __shfl_sync(0xffffffffu, b0, src);
+      const int j1 = __shfl_sync(0xffffffffu, b1, src);
+      const double ox = shfl_d(off[0], src), oy = shfl_d(off[1], src), oz = shfl_d(off[2], src);
+      int32_t cshift[3];
+      cshift[0] = __shfl_sync(0xffffffffu, sh[0], src);
+      cshift[1] = __shfl_sync(0xffffffffu, sh[1], src);
+      cshift[2] = __shfl_sync(0xffffffffu, sh[2], src);
+      const bool shifted = (cshift[0] | cshift[1] | cshift[2]) != 0;
+      for (int jb = j0; jb < j1; jb += 32) {
+        const int j = jb + lane;
+        bool hit = false;
+        double d2 = 0.0;
+        int32_t jo = 0;
+        int32_t s[3] = {0, 0, 0};
+        if (j < j1) {
+          const double dx = dadd(dsub(v.px[j], pix), ox);
+          const double dy = dadd(dsub(v.py[j], piy), oy);
+          const double dz = dadd(dsub(v.pz[j], piz), oz);
+          d2 = norm2(dx, dy, dz);
+          const SlotMeta mj = v.meta[j];
+          jo = mj.orig;
+          hit = d2 < max_sq && (mi.orig < jo || (mi.orig == jo && shifted));
+          s[0] = (mj.sx - mi.sx) + cshift[0];
+          s[1] = (mj.sy - mi.sy) + cshift[1];
+          s[2] = (mj.sz - mi.sz) + cshift[2];
+        }
+        sink(hit, d2, mi.orig, jo, s);
+      }
+    }
+  }
+}
+
+template <class Sink>
+__device__ __forceinline__ void visit_smem_brute_atom(const SysPlan& P, const SmemView& v, int i,
+                                                      double max_sq, Sink& sink) {
+  const int lane = threadIdx.x & 31;
+  const int n = P.n;
+  const double xi = v.px[i], yi = v.py[i], zi = v.pz[i];
+  for (int jb = i + 1; jb < n; jb += 32) {
+    const int j = jb + lane;
+    bool hit = false;
+    double d2 = 0.0;
+    int32_t s[3] = {0, 0, 0};
+    if (j < n) {
+      const double xj = v.px[j], yj = v.py[j], zj = v.pz[j];
+      if (P.method == 0) {
+        d2 = norm2(dsub(xj, xi), dsub(yj, yi), dsub(zj, zi));
+      } else {
+        double df[3];
+        matvec(P.g.hinv, dsub(xj, xi), dsub(yj, yi), dsub(zj, zi), df);
+        double sf[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          sf[a] = P.pbc[a] ? -round(df[a]) : 0.0;
+          s[a] = sat_i32(sf[a]);
+        }
+        double hv[3];
+        matvec(P.g.h, sf[0], sf[1], sf[2], hv);
+        d2 = norm2(dsub(dadd(xj, hv[0]), xi), dsub(dadd(yj, hv[1]), yi), dsub(dadd(zj, hv[2]), zi));
+      }
+      hit = d2 < max_sq;
+    }
+    sink(hit, d2, i, j, s);
+  }
+}
+
+// Pulls the next system index (in work order) for the whole CTA; -1 when done.
+__device__ __forceinline__ int next_system(int* work, const int32_t* order, int n_sys) {
+  __shared__ int s_next;
+  if (threadIdx.x == 0) s_next = atomicAdd(work, 1);
+  __syncthreads();
+  const int w = s_next;
+  __syncthreads();
+  return w < n_sys ? order[w] : -1;
+}
+
+__device__ __forceinline__ void load_plan(const SysPlan* plans, int s, SysPlan& sp_smem) {
+  const int words = (int)(sizeof(SysPlan) / sizeof(int32_t));
+  const int32_t* src = reinterpret_cast<const int32_t*>(plans + s);
+  int32_t* dst = reinterpret_cast<int32_t*>(&sp_smem);
+  for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBatchThreads)
+    k_batch_count(const SysPlan* __restrict__ plans, const int32_t* __restrict__ order, int n_sys,
+                  const double* __restrict__ pos, int cap, CutoffSet cs,
+                  uint32_t* __restrict__ counts, int64_t row, int* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ SysPlan P;
+  const SmemView v = smem_view(smem, cap);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    const int s = next_system(work, order, n_sys);
+    if (s < 0) break;
+    load_plan(plans, s, P);
+    if (P.method < 0) continue;
+    load_system(P, pos, v);
+    for (int p = warp; p < P.n; p += kBatchWarps) {
+      CountSink sink{&cs, 0u};
+      if (P.method == 2)
+        visit_smem_grid_atom(P, v, p, cs.max_sq, sink);
+      else
+        visit_smem_brute_atom(P, v, p, cs.max_sq, sink);
+      if (lane < cs.k) counts[(int64_t)lane * row + P.slot + p] = sink.cnt;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kBatchThreads)
+    k_batch_emit(const SysPlan* __restrict__ plans, const int32_t* __restrict__ order, int n_sys,
+                 const double* __restrict__ pos, int cap, CutoffSet cs,
+                 const int64_t* __restrict__ offs, int64_t row, EmitTargets t,
+                 int* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ SysPlan P;
+  const SmemView v = smem_view(smem, cap);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    const int s = next_system(work, order, n_sys);
+    if (s < 0) break;
+    load_plan(plans, s, P);
+    if (P.method < 0) continue;
+    load_system(P, pos, v);
+    for (int p = warp; p < P.n; p += kBatchWarps) {
+      int64_t cur = 0;
+      if (lane < cs.k) {
+        const int64_t r = (int64_t)lane * row;
+        cur = t.base[lane] + (offs[r + P.slot + p] - offs[r]);
+      }
+      EmitSink sink{&cs, &t, cur, P.start};
+      if (P.method == 2)
+        visit_smem_grid_atom(P, v, p, cs.max_sq, sink);
+      else
+        visit_smem_brute_atom(P, v, p, cs.max_sq, sink);
+    }
+    __syncthreads();
+  }
+}
+
+int grid_for(const void* func, size_t smem) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kBatchThreads, smem);
+  if (per_sm < 1) per_sm = 1;
+  return sms * per_sm;
+}
+
+}  // namespace
+
+size_t batch_smem_bytes(int cap) {
+  return (size_t)cap * (2 * sizeof(uint64_t) + 3 * sizeof(double) + sizeof(SlotMeta) +
+                        sizeof(int32_t));
+}
+
+void launch_plan(const double* pos, const int64_t* starts, int32_t s0, int32_t s1,
+                 const double* cells, const uint8_t* pbcs, const uint8_t* has_cell, double rc_max,
+                 uint64_t bf_threshold, int multi, int64_t run_start, SysPlan* plans,
+                 int32_t* error_flag, cudaStream_t s) {
+  const int per_block = 8;
+  const unsigned blocks = (unsigned)((s1 - s0 + per_block - 1) / per_block);
+  k_plan<<<blocks, per_block * 32, 0, s>>>(pos, starts, s0, s1, cells, pbcs, has_cell, rc_max,
+                                           bf_threshold, multi, run_start, plans, error_flag);
+  note_launches(1);
+}
+
+void launch_batch_count(const SysPlan* plans, const int32_t* order, int n_sys, const double* pos,
+                        int cap, const CutoffSet& cs, uint32_t* counts, int64_t row, int* work,
+                        cudaStream_t s) {
+  const size_t smem = batch_smem_bytes(cap);
+  ensure_smem_attr((const void*)k_batch_count, (int)smem);
+  const int grid = std::min(grid_for((const void*)k_batch_count, smem), std::max(n_sys, 1));
+  k_batch_count<<<grid, kBatchThreads, smem, s>>>(plans, order, n_sys, pos, cap, cs, counts, row,
+                                                  work);
+  note_launches(1);
+}
+
+void launch_batch_emit(const SysPlan* plans, const int32_t* order, int n_sys, const double* pos,
+                       int cap, const CutoffSet& cs, const int64_t* offs, int64_t row,
+                       const EmitTargets& t, int* work, cudaStream_t s) {
+  const size_t smem = batch_smem_bytes(cap);
+  ensure_smem_attr((const void*)k_batch_emit, (int)smem);
+  const int grid = std::min(grid_for((const void*)k_batch_emit, smem), std::max(n_sys, 1));
+  k_batch_emit<<<grid, kBatchThreads, smem, s>>>(plans, order, n_sys, pos, cap, cs, offs, row, t,
+                                                 work);
+  note_launches(1);
+}
+
+}  // namespace nlb

@@ -17,73 +17,13 @@
 // Brute force (src/search.rs:1187-1405): the same warp machinery with
 // candidates j = i+1..n-1 in index order, on raw positions (isolated) or with
 // the round-based minimum image (src/cell.rs:74-93).
-#include "nlb_kernels.h"
+#include "k_traverse.cuh"
 
 namespace nlb {
 
 namespace {
 
 constexpr int kWarpsPerBlock = 8;
-
-__device__ __forceinline__ unsigned lanemask_lt() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-__device__ __forceinline__ double shfl_d(double v, int src) {
-  return __shfl_sync(0xffffffffu, v, src);
-}
-
-// Hit sink for the count pass: lane q accumulates cutoff q's count.
-struct CountSink {
-  const CutoffSet* cs;
-  uint32_t cnt;  // lane q: count of cutoff q
-  __device__ __forceinline__ void operator()(bool hit, double d2, int32_t, int32_t, const int32_t*) {
-    const int lane = threadIdx.x & 31;
-    const int k = cs->k;
-    double prev = cs->lower_sq;
-    for (int q = 0; q < k; ++q) {
-      const double rq = cs->rc_sq[q];
-      const bool h = hit && d2 < rq && !(cs->disjoint && d2 < prev);
-      const unsigned m = __ballot_sync(0xffffffffu, h);
-      if (lane == q) cnt += __popc(m);
-      prev = rq;
-    }
-  }
-};
-
-// Hit sink for the emit pass: lane q holds cutoff q's next write slot.
-struct EmitSink {
-  const CutoffSet* cs;
-  const EmitTargets* t;
-  int64_t cursor;  // lane q: next slot of cutoff q
-  __device__ __forceinline__ void operator()(bool hit, double d2, int32_t io, int32_t jo,
-                                             const int32_t* s) {
-    const int lane = threadIdx.x & 31;
-    const int k = cs->k;
-    double prev = cs->lower_sq;
-    for (int q = 0; q < k; ++q) {
-      const double rq = cs->rc_sq[q];
-      const bool h = hit && d2 < rq && !(cs->disjoint && d2 < prev);
-      const unsigned m = __ballot_sync(0xffffffffu, h);
-      if (m) {
-        const int64_t c = __shfl_sync(0xffffffffu, cursor, q);
-        if (h) {
-          const int64_t e = c + __popc(m & lanemask_lt());
-          t->src[q][e] = (int64_t)io + t->index_offset;
-          t->dst[q][e] = (int64_t)jo + t->index_offset;
-          int32_t* sh = t->sh[q] + 3 * e;
-          sh[0] = s[0];
-          sh[1] = s[1];
-          sh[2] = s[2];
-        }
-        if (lane == q) cursor += __popc(m);
-      }
-      prev = rq;
-    }
-  }
-};
 
 // Visits sorted atom p's candidates in canonical order; all 32 lanes call
 // sink(hit, d2, i_orig, j_orig, shift) once per candidate step.
@@ -196,7 +136,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     const int64_t row = (int64_t)lane * (n + 1);
     cur = t.base[lane] + (offs[row + p] - offs[row]);
   }
-  EmitSink sink{&cs, &t, cur};
+  EmitSink sink{&cs, &t, cur, t.index_offset};
   visit_grid_atom(g, b, p, cs.max_sq, sink);
 }
 
@@ -258,7 +198,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
     const int64_t row = (int64_t)lane * (n + 1);
     cur = t.base[lane] + (offs[row + i] - offs[row]);
   }
-  EmitSink sink{&cs, &t, cur};
+  EmitSink sink{&cs, &t, cur, t.index_offset};
   visit_brute_atom(bp, pos, n, i, cs.max_sq, sink);
 }
 

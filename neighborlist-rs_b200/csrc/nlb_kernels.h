@@ -75,6 +75,34 @@ void launch_brute_count(const BruteParams& bp, const double* pos, int64_t n, con
 void launch_brute_emit(const BruteParams& bp, const double* pos, int64_t n, const CutoffSet& cs,
                        const int64_t* offs, const EmitTargets& t, cudaStream_t s);
 
+// ---- k_batch.cu : many small systems per launch (one CTA per system)
+constexpr int kBatchMaxAtoms = 2048;  // larger systems take the single-system pipeline
+
+struct SysPlan {
+  GridParams g;      // h / hinv always; grid fields for the cell-list method
+  int32_t pbc[3];
+  int32_t method;    // 0 brute force (raw), 1 brute force (MIC), 2 cell list, -1 invalid cell
+  int64_t start;     // first atom of the system (global index)
+  int32_t n;         // atoms
+  int32_t slot;      // first count slot of the system inside its run
+};
+
+size_t batch_smem_bytes(int cap);
+// Plans systems [s0, s1): plans[s - s0].  error_flag: 1 = singular cell,
+// 2 = stencil too large.
+void launch_plan(const double* pos, const int64_t* starts, int32_t s0, int32_t s1,
+                 const double* cells, const uint8_t* pbcs, const uint8_t* has_cell, double rc_max,
+                 uint64_t bf_threshold, int multi, int64_t run_start, SysPlan* plans,
+                 int32_t* error_flag, cudaStream_t s);
+// counts[q * row + slot + p]; `work` must be zero on entry; cap = power of two
+// >= the largest system of the run.
+void launch_batch_count(const SysPlan* plans, const int32_t* order, int n_sys, const double* pos,
+                        int cap, const CutoffSet& cs, uint32_t* counts, int64_t row, int* work,
+                        cudaStream_t s);
+void launch_batch_emit(const SysPlan* plans, const int32_t* order, int n_sys, const double* pos,
+                       int cap, const CutoffSet& cs, const int64_t* offs, int64_t row,
+                       const EmitTargets& t, int* work, cudaStream_t s);
+
 // Sets the dynamic shared-memory limit of a kernel once per device.
 void ensure_smem_attr(const void* func, int bytes);
 

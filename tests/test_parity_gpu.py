@@ -206,3 +206,62 @@ def test_non_contiguous_inputs(nl):
     bl = np.zeros(200, np.int32)
     r = nl.build_neighborlists_batch(big[:50, :3], bl[::2][:50], None, 1.5)
     assert r["edge_index"].shape[0] == 2
+
+
+def test_batch_mixed_sizes_and_many_cutoffs(nl, oracle):
+    """Runs of small systems (batched kernels) around a system above the
+    batched-kernel size (single-system pipeline), plus > 32 cutoffs."""
+    from neighborlist_rs import workloads as W
+
+    small = W.uneven_batch(n_systems=10, seed=41)
+    rng = np.random.default_rng(42)
+    big_rows = np.diag([25.0, 25.0, 25.0])
+    big = W.System(rng.random((3000, 3)) @ big_rows, big_rows, 5.0)
+    iso_big = W.System(rng.random((2500, 3)) * 30.0, None, 5.0)
+    systems = small[:4] + [big] + small[4:7] + [iso_big] + small[7:]
+    pos, batch, cells = W.concat_batch(systems)
+    ocells = [None if not c.any() else (c.T, PBC3) for c in cells]
+    got = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=5.0)
+    (ref,) = oracle.search_batch(pos, batch, ocells, [5.0], nthreads=8)
+    assert_same(got, ref, "mixed small/large batch")
+    cs = list(np.linspace(1.5, 5.0, 35))
+    for dj in (False, True):
+        gm = nl.build_neighborlists_batch_multi(pos, batch, cells=cells, cutoffs=cs, disjoint=dj)
+        rm = oracle.search_batch(pos, batch, ocells, cs, disjoint=dj, nthreads=8)
+        for q in range(len(cs)):
+            assert_same(gm[q], rm[q], f"batch 35 cutoffs disjoint={dj} q={q}")
+
+
+def test_batch_singular_cell(nl):
+    pos = np.random.default_rng(1).random((6, 3))
+    batch = np.array([0, 0, 0, 1, 1, 1], np.int32)
+    cells = np.zeros((2, 3, 3))
+    cells[0] = np.eye(3) * 5.0
+    cells[1] = [[1.0, 0, 0], [2.0, 0, 0], [0, 0, 1.0]]   # singular
+    with pytest.raises(ValueError, match="Cell matrix is not invertible"):
+        nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=2.0)
+
+
+def test_batch_thresholds_and_self_images(nl, oracle):
+    """Tiny periodic boxes (many images, nb = 1) and the brute-force threshold
+    moved, inside the batched kernels."""
+    from neighborlist_rs import workloads as W
+
+    rng = np.random.default_rng(8)
+    systems = []
+    for s in range(40):
+        n = int(rng.integers(1, 30))
+        rows = W.density_cell(n, 0.1, rng, (75.0, 105.0))
+        systems.append(W.System(rng.random((n, 3)) @ rows, rows, 6.0))
+    pos, batch, cells = W.concat_batch(systems)
+    ocells = [(c.T, PBC3) for c in cells]
+    for bf in (1000, 0, 20):
+        nl.set_brute_force_threshold(bf)
+        oracle.set_thresholds(bf, 300)
+        try:
+            got = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=6.0)
+            (ref,) = oracle.search_batch(pos, batch, ocells, [6.0], nthreads=8)
+            assert_same(got, ref, f"tiny boxes, brute-force threshold {bf}")
+        finally:
+            nl.set_brute_force_threshold(1000)
+            oracle.set_thresholds(1000, 300)
