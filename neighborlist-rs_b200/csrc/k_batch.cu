@@ -103,6 +103,7 @@ __device__ void dev_plan_grid(const double* w, double rc, GridParams& g) {
   d[3] = norm2(t[0], t[1], t[2]);
   const double mx = dfmax(dfmax(dfmax(d[0], d[1]), d[2]), d[3]);
   const double radius = dmul(0.5, __dsqrt_rn(mx));
+  g.radius = radius;
   const double pl = dadd(__dsqrt_rn(dmul(rc, rc)), radius);
   g.prune_sq = dmul(pl, pl);
 }

@@ -130,7 +130,9 @@ __global__ void __launch_bounds__(kSortThreads)
               uint64_t* __restrict__ skey, int32_t* __restrict__ sidx,
               uint64_t* __restrict__ skey2, int32_t* __restrict__ sidx2,
               double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz,
-              SlotMeta* __restrict__ meta) {
+              SlotMeta* __restrict__ meta, float4* __restrict__ p32, int32_t* __restrict__ sbin,
+              int2* __restrict__ groups, int32_t* __restrict__ irr_list,
+              uint8_t* __restrict__ irr, int32_t* __restrict__ counters) {
   __shared__ uint64_t sk[kSortCap];
   __shared__ int32_t sv[kSortCap];
   const int64_t r = blockIdx.x;
@@ -209,6 +211,38 @@ __global__ void __launch_bounds__(kSortThreads)
     mt.sz = w.s[2];
     mt.orig = idx;
     meta[p] = mt;
+    if (p32) {
+      // Bin centre of the stored bin (same expression as the prune test's
+      // target centre, src/search.rs:493-497).
+      double c[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double t = dadd(g.origin[k], dmul(g.basis[0][k], (double)w.bin[0]));
+        t = dadd(t, dmul(g.basis[1][k], (double)w.bin[1]));
+        c[k] = dadd(t, dmul(g.basis[2][k], (double)w.bin[2]));
+      }
+      p32[p] = make_float4(__double2float_rn(dsub(w.wx, c[0])), __double2float_rn(dsub(w.wy, c[1])),
+                           __double2float_rn(dsub(w.wz, c[2])), __int_as_float(idx));
+      sbin[p] = w.bin[0] + g.nb[0] * (w.bin[1] + g.nb[1] * w.bin[2]);
+      // Home stencil centre, recomputed from the wrapped position exactly as
+      // the search does (src/search.rs:454-457).
+      double fi[3];
+      matvec(g.hinv, w.wx, w.wy, w.wz, fi);
+      bool same = true;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int32_t v = sat_i32(dmul(fi[a], (double)g.nb[a]));
+        const int32_t hb = v < g.nb[a] - 1 ? v : g.nb[a] - 1;
+        same = same && hb == w.bin[a];
+      }
+      irr[p] = same ? 0 : 1;
+      if (!same) irr_list[atomicAdd(&counters[1], 1)] = (int32_t)p;
+    }
+  }
+  if (p32 && threadIdx.x == 0) {
+    const int ng = (int)((cnt + 31) / 32);
+    const int base = atomicAdd(&counters[0], ng);
+    for (int k = 0; k < ng; ++k) groups[base + k] = make_int2((int)(s + 32 * k), (int)r);
   }
 }
 
@@ -261,17 +295,21 @@ void launch_bounds(const double* pos, int64_t n, double* out, cudaStream_t s) {
 }
 
 void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const GridBuffers& b,
-                       cudaStream_t s) {
+                       cudaStream_t s, bool need_rank_table) {
   const int T = 256;
-  k_rank_table<<<(unsigned)((g.total_bins + T - 1) / T), T, 0, s>>>(g, b.rank_of_bin);
+  if (need_rank_table) {
+    k_rank_table<<<(unsigned)((g.total_bins + T - 1) / T), T, 0, s>>>(g, b.rank_of_bin);
+    note_launches(1);
+  }
   k_prep<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(g, pos, n, b.rank_of_bin, b.key, b.rank,
                                                     b.bin_count);
   exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
   k_scatter<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(b.key, b.rank, n, b.bin_start, b.bin_fill,
                                                        b.skey, b.sidx);
   k_binsort<<<(unsigned)g.total_bins, kSortThreads, 0, s>>>(
-      g, pos, b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta);
-  note_launches(4);
+      g, pos, b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta, b.p32,
+      b.sbin, b.groups, b.irr_list, b.irr, b.counters);
+  note_launches(3);
 }
 
 }  // namespace nlb

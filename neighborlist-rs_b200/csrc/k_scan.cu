@@ -1,126 +1,180 @@
-// k_scan.cu -- exclusive prefix sums used by the count -> scan -> emit
-// pipeline (per-atom edge counts -> int64 edge offsets) and by the bin
-// histogram (bin counts -> bin starts).
+// k_scan.cu -- exclusive prefix sums (edge counts -> int64 edge offsets,
+// bin histogram -> bin starts) in ONE launch of any size.
 //
-// One tile = 1024 threads x 16 items.  Inputs up to one tile take a single
-// launch; larger inputs take three (tile scans, scan of tile totals, add).
-// Loads and stores are staged through shared memory so global accesses are
-// coalesced.  HBM-bound: 4 B read + 8 B written per element.
+// Single-pass scan with decoupled look-back: each CTA takes the next tile
+// ticket (so every tile it waits on belongs to a CTA that is already
+// running), scans its tile in shared memory, publishes its aggregate, then a
+// warp walks back over the predecessors' published aggregates / inclusive
+// prefixes 32 at a time until it meets an inclusive prefix.  Every wait is
+// bounded: after kSpinLimit polls the CTA records an error in the state
+// buffer (word 1, read back by the host) and stops waiting.  HBM-bound:
+// 4 B read + 8 B written per element.  The state buffer (tiles + 2 words) is
+// zeroed by a memset node right before the kernel.
 #include "nlb_kernels.h"
 
 namespace nlb {
 
 namespace {
 
-constexpr int kThreads = 1024;
+constexpr int kThreads = 256;
 constexpr int kItems = 16;
-constexpr int64_t kTile = (int64_t)kThreads * kItems;
+constexpr int kTile = kThreads * kItems;  // 4096 elements
+constexpr int kPadShift = 5;              // one padding word per 32 elements
+constexpr int kSpinLimit = 1 << 22;
 
-// Exclusive scan of one value per thread across the block; returns the
-// exclusive prefix and writes the block total to *total.
-__device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t* total) {
-  __shared__ int64_t warp_sums[32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int64_t x = v;
+constexpr uint64_t kStatusShift = 62;
+constexpr uint64_t kAggregate = 1ull << kStatusShift;
+constexpr uint64_t kInclusive = 2ull << kStatusShift;
+constexpr uint64_t kValueMask = (1ull << kStatusShift) - 1;
+
+__device__ __forceinline__ int pad(int i) { return i + (i >> kPadShift); }
+
+__device__ __forceinline__ uint64_t load_state(const uint64_t* p) {
+  return *reinterpret_cast<const volatile uint64_t*>(p);
+}
+
+__device__ __forceinline__ void store_state(uint64_t* p, uint64_t v) {
+  __threadfence();
+  *reinterpret_cast<volatile uint64_t*>(p) = v;
+}
+
+template <class TIn>
+__global__ void __launch_bounds__(kThreads)
+    k_scan(const TIn* __restrict__ in, int64_t n, int64_t* __restrict__ out,
+           uint64_t* __restrict__ state) {
+  // state[0]: tile ticket counter; state[1]: error flag; state[2 + t]: tile t.
+  __shared__ uint32_t stage_in[kTile + kTile / 32];
+  __shared__ int64_t warp_sums[kThreads / 32];
+  __shared__ int64_t s_prefix;
+  __shared__ int s_tile;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = (int)atomicAdd(reinterpret_cast<unsigned long long*>(&state[0]), 1ull);
+  __syncthreads();
+  const int tile = s_tile;
+  const int64_t base = (int64_t)tile * kTile;
+
+  // Coalesced load into padded shared memory; each thread then owns kItems
+  // consecutive elements.
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const int i = k * kThreads + tid;
+    const int64_t g = base + i;
+    stage_in[pad(i)] = g < n ? (uint32_t)in[g] : 0u;
+  }
+  __syncthreads();
+  int64_t local[kItems];
+  int64_t sum = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    local[k] = sum;
+    sum += stage_in[pad(tid * kItems + k)];
+  }
+  // Block exclusive scan of the per-thread sums.
+  int64_t x = sum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
     if (lane >= o) x += y;
   }
   if (lane == 31) warp_sums[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    const int nw = blockDim.x >> 5;
-    int64_t s = lane < nw ? warp_sums[lane] : 0;
+    int64_t w = lane < kThreads / 32 ? warp_sums[lane] : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int64_t y = __shfl_up_sync(0xffffffffu, s, o);
-      if (lane >= o) s += y;
+      const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
     }
-    if (lane < nw) warp_sums[lane] = s;
+    if (lane < kThreads / 32) warp_sums[lane] = w;
   }
   __syncthreads();
-  const int64_t warp_prefix = warp ? warp_sums[warp - 1] : 0;
-  *total = warp_sums[(blockDim.x >> 5) - 1];
-  __syncthreads();
-  return warp_prefix + x - v;
-}
+  const int64_t aggregate = warp_sums[kThreads / 32 - 1];
+  const int64_t thread_prefix = (warp ? warp_sums[warp - 1] : 0) + x - sum;
 
-template <class TIn>
-__global__ void __launch_bounds__(kThreads) scan_tiles(const TIn* __restrict__ in, int64_t n,
-                                                       int64_t* __restrict__ out,
-                                                       int64_t* __restrict__ tile_totals) {
-  extern __shared__ int64_t stage[];  // kTile items (128 KB, dynamic)
-  const int64_t base = (int64_t)blockIdx.x * kTile;
-  for (int k = 0; k < kItems; ++k) {
-    const int64_t i = base + (int64_t)k * kThreads + threadIdx.x;
-    stage[k * kThreads + threadIdx.x] = i < n ? (int64_t)in[i] : 0;
-  }
-  __syncthreads();
-  int64_t loc[kItems];
-  int64_t sum = 0;
+  // Decoupled look-back (warp 0).
+  if (warp == 0) {
+    uint64_t* tiles = state + 2;
+    int64_t prefix = 0;
+    if (tile == 0) {
+      if (lane == 0) store_state(&tiles[0], kInclusive | ((uint64_t)aggregate & kValueMask));
+    } else {
+      if (lane == 0) store_state(&tiles[tile], kAggregate | ((uint64_t)aggregate & kValueMask));
+      int t = tile - 1;
+      for (;;) {
+        const int pred = t - lane;  // lane 0 = nearest predecessor
+        uint64_t v = kInclusive;    // lanes before tile 0 act as an empty prefix
+        bool failed = false;
+        if (pred >= 0) {
+          int spins = 0;
+          v = load_state(&tiles[pred]);
+          while ((v >> kStatusShift) == 0 && spins < kSpinLimit) {
+            __nanosleep(32);
+            v = load_state(&tiles[pred]);
+            ++spins;
+          }
+          failed = (v >> kStatusShift) == 0;
+        }
+        if (__any_sync(0xffffffffu, failed)) {
+          if (lane == 0) atomicExch(reinterpret_cast<unsigned long long*>(&state[1]), 1ull);
+          break;
+        }
+        const bool inc = (v >> kStatusShift) == 2;
+        const unsigned inc_mask = __ballot_sync(0xffffffffu, inc);
+        const int stop = __ffs(inc_mask) - 1;  // nearest inclusive prefix in this window
+        int64_t val = (pred >= 0 && lane <= (stop < 0 ? 31 : stop)) ? (int64_t)(v & kValueMask) : 0;
 #pragma unroll
-  for (int k = 0; k < kItems; ++k) {
-    loc[k] = sum;
-    sum += stage[threadIdx.x * kItems + k];
+        for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+        prefix += val;
+        if (stop >= 0) break;
+        t -= 32;
+      }
+      if (lane == 0)
+        store_state(&tiles[tile], kInclusive | ((uint64_t)(prefix + aggregate) & kValueMask));
+    }
+    if (lane == 0) s_prefix = prefix;
   }
-  int64_t total;
-  const int64_t pre = block_exclusive_scan(sum, &total);
-#pragma unroll
-  for (int k = 0; k < kItems; ++k) stage[threadIdx.x * kItems + k] = pre + loc[k];
   __syncthreads();
-  for (int k = 0; k < kItems; ++k) {
-    const int64_t i = base + (int64_t)k * kThreads + threadIdx.x;
-    if (i < n) out[i] = stage[k * kThreads + threadIdx.x];
+  const int64_t prefix = s_prefix;
+
+  // Results go out through shared memory in two halves so the global stores
+  // are coalesced (the int64 stage reuses the input stage's space).
+  int64_t* stage_out = reinterpret_cast<int64_t*>(stage_in);
+  constexpr int kHalf = kTile / 2;
+  for (int h = 0; h < 2; ++h) {
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      const int i = tid * kItems + k;
+      if (i >= h * kHalf && i < (h + 1) * kHalf) {
+        const int li = i - h * kHalf;
+        stage_out[li + (li >> kPadShift)] = prefix + thread_prefix + local[k];
+      }
+    }
+    __syncthreads();
+    for (int li = tid; li < kHalf; li += kThreads) {
+      const int64_t g = base + h * kHalf + li;
+      if (g < n) out[g] = stage_out[li + (li >> kPadShift)];
+    }
   }
-  if (threadIdx.x == 0) {
-    if (tile_totals) tile_totals[blockIdx.x] = total;
-    if (gridDim.x == 1) out[n] = total;
-  }
+  const int64_t last_tile = n > 0 ? (n - 1) / kTile : 0;
+  if (tid == 0 && tile == last_tile) out[n] = prefix + aggregate;
 }
 
-__global__ void __launch_bounds__(kThreads) add_tile_bases(int64_t* __restrict__ out, int64_t n,
-                                                           const int64_t* __restrict__ bases) {
-  const int64_t base = (int64_t)blockIdx.x * kTile;
-  const int64_t add = bases[blockIdx.x];
-  for (int k = 0; k < kItems; ++k) {
-    const int64_t i = base + (int64_t)k * kThreads + threadIdx.x;
-    if (i < n) out[i] += add;
-  }
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = bases[gridDim.x];
-}
-
-constexpr size_t kStageBytes = sizeof(int64_t) * kTile;
+static_assert(sizeof(int64_t) * ((kTile / 2) + (kTile / 2) / 32) <=
+                  sizeof(uint32_t) * (kTile + kTile / 32),
+              "the output stage must fit in the input stage");
 
 template <class TIn>
 void scan_impl(const TIn* in, int64_t n, int64_t* out, int64_t* tmp, cudaStream_t s) {
-  ensure_smem_attr((const void*)scan_tiles<TIn>, (int)kStageBytes);
-  const int64_t tiles = (n + kTile - 1) / kTile;
-  if (tiles <= 1) {
-    scan_tiles<TIn><<<1, kThreads, kStageBytes, s>>>(in, n, out, nullptr);
-    note_launches(1);
-    return;
-  }
-  // tmp layout: [tile totals (tiles)] [scanned totals (tiles + 1)] [scratch...]
-  int64_t* totals = tmp;
-  int64_t* bases = tmp + tiles;
-  scan_tiles<TIn><<<(unsigned)tiles, kThreads, kStageBytes, s>>>(in, n, out, totals);
-  scan_impl<int64_t>(totals, tiles, bases, tmp + 2 * tiles + 1, s);
-  add_tile_bases<<<(unsigned)tiles, kThreads, 0, s>>>(out, n, bases);
-  note_launches(2);
+  const int64_t tiles = n > 0 ? (n + kTile - 1) / kTile : 1;
+  cudaMemsetAsync(tmp, 0, sizeof(int64_t) * (size_t)(tiles + 2), s);
+  k_scan<TIn><<<(unsigned)tiles, kThreads, 0, s>>>(in, n, out, reinterpret_cast<uint64_t*>(tmp));
+  note_launches(1);
 }
 
 }  // namespace
 
-int64_t scan_tmp_elems(int64_t n) {
-  int64_t need = 0;
-  while (n > kTile) {
-    const int64_t tiles = (n + kTile - 1) / kTile;
-    need += 2 * tiles + 1;
-    n = tiles;
-  }
-  return need + 1;
-}
+int64_t scan_tmp_elems(int64_t n) { return (n > 0 ? (n + kTile - 1) / kTile : 1) + 2; }
 
 void exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, int64_t* tmp,
                         cudaStream_t s) {

@@ -1,0 +1,299 @@
+// k_search2.cu -- single-cutoff stencil search as (atom group, stencil cell)
+// pair tasks, with an FP32 pair test and an exact FP64 guard-band recheck.
+//
+// Same edges, same order as k_search.cu and the reference.  The canonical
+// order is (sorted atom, stencil cell in x/y/z order, candidate in bin
+// order), so per-(atom, cell) edge counts, scanned in that order, give every
+// (atom, cell) its exact output offset and all tasks can run in parallel:
+//
+// * A task is one group of at most 32 atoms of one bin (lane = atom) and one
+//   stencil cell.  The cell (periodic bin, image shift, FP64 image offset,
+//   bin range) is shared by the group; each lane applies the reference's
+//   FP64 prune test for its own atom (src/search.rs:500-505).
+// * The cell's candidates are staged 32 at a time in shared memory as FP32
+//   positions relative to their bin centre (original index in .w); each lane
+//   tests them in bin order against its atom: dx = x_j + (T - x_i) with the
+//   cell translation T = c_cell + off - c_bin formed in FP64 and rounded once.
+// * Guard band (make_guard_band): d2_32 < rc^2 - delta is a certain hit,
+//   d2_32 >= rc^2 + delta a certain miss; in between, the reference's exact
+//   FP64 expression (x_j - x_i) + off on the FP64 wrapped positions decides
+//   (src/search.rs:540-553).  Results are identical to the FP64 kernels.
+// * Atoms whose home stencil differs from their stored bin (the search
+//   recomputes the home bin from the wrapped position, src/search.rs:454-457;
+//   this differs only within rounding of a bin face) are skipped by the
+//   tasks and handled by one warp each, in FP64, with the same outputs.
+#include <cmath>
+
+#include "k_traverse.cuh"
+
+namespace nlb {
+
+namespace {
+
+constexpr int kPairWarps = 8;  // warps per CTA
+
+struct CellDesc {
+  int32_t b0, b1;  // candidate slots
+  int32_t sh[3];   // image shift
+  double off[3];   // image offset (FP64, reference order)
+  double cs[3];    // bin centre + offset (FP64), the prune test's target
+};
+
+// Stencil cell c of the stencil centred on bin `home`.
+__device__ __forceinline__ CellDesc describe_cell(const GridParams& g, const GridBuffers& b,
+                                                  const int32_t home[3], int32_t c) {
+  const int32_t ny = 2 * g.ns[1] + 1, nz = 2 * g.ns[2] + 1;
+  const int32_t ix = c / (ny * nz);
+  const int32_t rem = c - ix * (ny * nz);
+  const int32_t iy = rem / nz, iz = rem - (rem / nz) * nz;
+  CellDesc d;
+  int32_t bin[3];
+  div_mod(home[0] + ix - g.ns[0], g.nb[0], bin[0], d.sh[0]);
+  div_mod(home[1] + iy - g.ns[1], g.nb[1], bin[1], d.sh[1]);
+  div_mod(home[2] + iz - g.ns[2], g.nb[2], bin[2], d.sh[2]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    d.off[k] = dadd(dadd(dmul(g.h[3 * k], (double)d.sh[0]), dmul(g.h[3 * k + 1], (double)d.sh[1])),
+                    dmul(g.h[3 * k + 2], (double)d.sh[2]));
+    double t = dadd(g.origin[k], dmul(g.basis[0][k], (double)bin[0]));
+    t = dadd(t, dmul(g.basis[1][k], (double)bin[1]));
+    t = dadd(t, dmul(g.basis[2][k], (double)bin[2]));
+    d.cs[k] = dadd(t, d.off[k]);
+  }
+  const int64_t lin = bin[0] + (int64_t)g.nb[0] * (bin[1] + (int64_t)g.nb[1] * bin[2]);
+  const int32_t r = b.rank_of_bin[lin];
+  d.b0 = (int32_t)b.bin_start[r];
+  d.b1 = (int32_t)b.bin_start[r + 1];
+  return d;
+}
+
+__device__ __forceinline__ void bin_centre(const GridParams& g, int32_t lin, double c[3]) {
+  const int32_t bx = lin % g.nb[0];
+  const int32_t by = (lin / g.nb[0]) % g.nb[1];
+  const int32_t bz = lin / (g.nb[0] * g.nb[1]);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    double v = dadd(g.origin[k], dmul(g.basis[0][k], (double)bx));
+    v = dadd(v, dmul(g.basis[1][k], (double)by));
+    c[k] = dadd(v, dmul(g.basis[2][k], (double)bz));
+  }
+}
+
+// One warp per irregular atom: every stencil cell of its own home stencil in
+// order, candidates 32 at a time across lanes (FP64, like k_search.cu).
+template <bool EMIT>
+__device__ void pair_irregular(const GridParams& g, const GridBuffers& b, int32_t n_cells,
+                               double rc_sq, uint32_t* __restrict__ counts,
+                               const int64_t* __restrict__ offs, const EmitTargets& t,
+                               int64_t gwarp, int64_t nwarps) {
+  const int lane = threadIdx.x & 31;
+  const int32_t n_irr = b.counters[1];
+  const int64_t off0 = EMIT ? offs[0] : 0;
+  for (int64_t w = gwarp; w < n_irr; w += nwarps) {
+    const int32_t p = b.irr_list[w];
+    const double xi = b.px[p], yi = b.py[p], zi = b.pz[p];
+    const SlotMeta mi = b.meta[p];
+    double fi[3];
+    matvec(g.hinv, xi, yi, zi, fi);
+    int32_t home[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int32_t v = sat_i32(dmul(fi[a], (double)g.nb[a]));
+      home[a] = v < g.nb[a] - 1 ? v : g.nb[a] - 1;
+    }
+    for (int32_t c = 0; c < n_cells; ++c) {
+      const CellDesc d = describe_cell(g, b, home, c);
+      const bool live = !(norm2(dsub(d.cs[0], xi), dsub(d.cs[1], yi), dsub(d.cs[2], zi)) > g.prune_sq);
+      const bool shifted = (d.sh[0] | d.sh[1] | d.sh[2]) != 0;
+      uint32_t cnt = 0;
+      int64_t slot = EMIT ? t.base[0] + (offs[(int64_t)p * n_cells + c] - off0) : 0;
+      if (live) {
+        for (int32_t jb = d.b0; jb < d.b1; jb += 32) {
+          const int32_t j = jb + lane;
+          bool hit = false;
+          int32_t jo = 0;
+          SlotMeta mj{};
+          if (j < d.b1) {
+            const double ex = dadd(dsub(b.px[j], xi), d.off[0]);
+            const double ey = dadd(dsub(b.py[j], yi), d.off[1]);
+            const double ez = dadd(dsub(b.pz[j], zi), d.off[2]);
+            mj = b.meta[j];
+            jo = mj.orig;
+            hit = norm2(ex, ey, ez) < rc_sq && (mi.orig < jo || (mi.orig == jo && shifted));
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, hit);
+          if (!EMIT) {
+            cnt += __popc(m);
+          } else {
+            if (hit) {
+              const int64_t e = slot + __popc(m & lanemask_lt());
+              t.src[0][e] = (int64_t)mi.orig + t.index_offset;
+              t.dst[0][e] = (int64_t)jo + t.index_offset;
+              int32_t* sp = t.sh[0] + 3 * e;
+              sp[0] = (mj.sx - mi.sx) + d.sh[0];
+              sp[1] = (mj.sy - mi.sy) + d.sh[1];
+              sp[2] = (mj.sz - mi.sz) + d.sh[2];
+            }
+            slot += __popc(m);
+          }
+        }
+      }
+      if (!EMIT && lane == 0) counts[(int64_t)p * n_cells + c] = cnt;
+    }
+  }
+}
+
+template <bool EMIT>
+__global__ void __launch_bounds__(kPairWarps * 32)
+    k_pair_tasks(GridParams g, GridBuffers b, int64_t n, int32_t n_cells, GuardBand band,
+                 uint32_t* __restrict__ counts, const int64_t* __restrict__ offs, EmitTargets t) {
+  __shared__ float4 stage_q[kPairWarps][32];
+  __shared__ SlotMeta stage_m[kPairWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float4* sq = stage_q[warp];
+  SlotMeta* smt = stage_m[warp];
+  const int64_t n_tasks = (int64_t)b.counters[0] * n_cells;
+  const int64_t step = (int64_t)gridDim.x * kPairWarps;
+  const int64_t off0 = EMIT ? offs[0] : 0;
+
+  for (int64_t task = (int64_t)blockIdx.x * kPairWarps + warp; task < n_tasks; task += step) {
+    const int32_t gi = (int32_t)(task / n_cells);
+    const int32_t c = (int32_t)(task - (int64_t)gi * n_cells);
+    const int2 grp = b.groups[gi];
+    const int32_t first = grp.x;
+    const int32_t bin_end = (int32_t)b.bin_start[grp.y + 1];
+    const int32_t len = bin_end - first < 32 ? bin_end - first : 32;
+    const int32_t p = first + (lane < len ? lane : 0);
+    const bool mine = lane < len && !b.irr[p];
+
+    // The group's bin (stored and home stencil centre for regular atoms).
+    const int32_t lin = b.sbin[first];
+    int32_t home[3];
+    home[0] = lin % g.nb[0];
+    home[1] = (lin / g.nb[0]) % g.nb[1];
+    home[2] = lin / (g.nb[0] * g.nb[1]);
+    const CellDesc d = describe_cell(g, b, home, c);
+    double cb[3];
+    bin_centre(g, lin, cb);
+
+    const double xi = b.px[p], yi = b.py[p], zi = b.pz[p];
+    const bool live =
+        mine && !(norm2(dsub(d.cs[0], xi), dsub(d.cs[1], yi), dsub(d.cs[2], zi)) > g.prune_sq);
+    uint32_t cnt = 0;
+    int64_t slot = 0;
+    if (EMIT && mine) slot = t.base[0] + (offs[(int64_t)p * n_cells + c] - off0);
+    if (__any_sync(0xffffffffu, live) && d.b1 > d.b0) {
+      const float4 a = b.p32[p];
+      const int32_t io = __float_as_int(a.w);
+      const float ux = __double2float_rn(dsub(d.cs[0], cb[0])) - a.x;
+      const float uy = __double2float_rn(dsub(d.cs[1], cb[1])) - a.y;
+      const float uz = __double2float_rn(dsub(d.cs[2], cb[2])) - a.z;
+      const bool shifted = (d.sh[0] | d.sh[1] | d.sh[2]) != 0;
+      SlotMeta mi;
+      if (EMIT) mi = b.meta[p];
+      for (int32_t jb = d.b0; jb < d.b1; jb += 32) {
+        const int32_t nj = d.b1 - jb < 32 ? d.b1 - jb : 32;
+        if (lane < nj) {
+          sq[lane] = b.p32[jb + lane];
+          if (EMIT) smt[lane] = b.meta[jb + lane];
+        }
+        __syncwarp();
+        for (int32_t jj = 0; jj < nj; ++jj) {
+          const float4 q = sq[jj];
+          const float dx = q.x + ux;
+          const float dy = q.y + uy;
+          const float dz = q.z + uz;
+          const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+          bool in = d2 < band.lo;
+          if (live && !in && d2 < band.hi) {
+            const int32_t j = jb + jj;
+            const double ex = dadd(dsub(b.px[j], xi), d.off[0]);
+            const double ey = dadd(dsub(b.py[j], yi), d.off[1]);
+            const double ez = dadd(dsub(b.pz[j], zi), d.off[2]);
+            in = norm2(ex, ey, ez) < band.rc_sq;
+          }
+          const int32_t jo = __float_as_int(q.w);
+          const bool hit = live && in && (io < jo || (io == jo && shifted));
+          if (!EMIT) {
+            cnt += hit ? 1u : 0u;
+          } else if (hit) {
+            const SlotMeta mj = smt[jj];
+            t.src[0][slot] = (int64_t)io + t.index_offset;
+            t.dst[0][slot] = (int64_t)jo + t.index_offset;
+            int32_t* sp = t.sh[0] + 3 * slot;
+            sp[0] = (mj.sx - mi.sx) + d.sh[0];
+            sp[1] = (mj.sy - mi.sy) + d.sh[1];
+            sp[2] = (mj.sz - mi.sz) + d.sh[2];
+            ++slot;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    if (!EMIT && mine) counts[(int64_t)p * n_cells + c] = cnt;
+  }
+  // Atoms whose home stencil is not their stored bin (normally none).
+  pair_irregular<EMIT>(g, b, n_cells, band.rc_sq, counts, offs, t,
+                       (int64_t)blockIdx.x * kPairWarps + warp, step);
+  if (!EMIT && blockIdx.x == 0 && threadIdx.x == 0) counts[n * (int64_t)n_cells] = 0;
+}
+
+int pair_grid(const void* func) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kPairWarps * 32, 0);
+  if (per_sm < 1) per_sm = 1;
+  return sms * per_sm;
+}
+
+inline int32_t stencil_cells(const GridParams& g) {
+  return (2 * g.ns[0] + 1) * (2 * g.ns[1] + 1) * (2 * g.ns[2] + 1);
+}
+
+}  // namespace
+
+bool make_guard_band(const GridParams& g, double rc, GuardBand& band) {
+  // FP32 unit roundoff.  A task's candidates lie in a cell that is not pruned
+  // for the lane's atom, so |c_cell + off - x_i| <= rc + R and
+  // |T| = |c_cell + off - c_bin| <= rc + 2R; bin-relative coordinates satisfy
+  // |x| <= R.  The FP32 roundings of x_j, x_i, T, T - x_i and x_j + (T - x_i)
+  // bound each component's error by u (7R + 3rc) for pairs with |d| <= rc
+  // (eps doubles it).  The FMA reduction adds at most 3u d2.  delta covers
+  // 2 sqrt(3) eps |d| + 3 eps^2 + 3u d2 with a factor 2, plus the FP64
+  // reference's own rounding.
+  const double u = std::ldexp(1.0, -24);
+  const double R = g.radius;
+  if (!std::isfinite(R) || !std::isfinite(rc) || R <= 0.0) return false;
+  const double eps = 2.0 * u * (7.0 * R + 3.0 * rc) + 1e-12;
+  const double r = rc + eps;
+  const double delta =
+      2.0 * (2.0 * std::sqrt(3.0) * eps * r + 3.0 * eps * eps + 4.0 * u * r * r) + 1e-12 * r * r;
+  const double rc2 = rc * rc;
+  if (!(delta < 1e-3 * rc2)) return false;
+  if (stencil_cells(g) > kPairMaxCells) return false;
+  band.rc_sq = rc2;
+  band.lo = std::nextafter((float)(rc2 - delta), -INFINITY);
+  band.hi = std::nextafter((float)(rc2 + delta), INFINITY);
+  return true;
+}
+
+void launch_pair_count(const GridParams& g, const GridBuffers& b, int64_t n,
+                       const GuardBand& band, uint32_t* counts, cudaStream_t s) {
+  EmitTargets t{};
+  const int32_t cells = stencil_cells(g);
+  k_pair_tasks<false><<<pair_grid((const void*)k_pair_tasks<false>), kPairWarps * 32, 0, s>>>(
+      g, b, n, cells, band, counts, nullptr, t);
+  note_launches(1);
+}
+
+void launch_pair_emit(const GridParams& g, const GridBuffers& b, int64_t n,
+                      const GuardBand& band, const int64_t* offs, const EmitTargets& t,
+                      cudaStream_t s) {
+  const int32_t cells = stencil_cells(g);
+  k_pair_tasks<true><<<pair_grid((const void*)k_pair_tasks<true>), kPairWarps * 32, 0, s>>>(
+      g, b, n, cells, band, nullptr, offs, t);
+  note_launches(1);
+}
+
+}  // namespace nlb

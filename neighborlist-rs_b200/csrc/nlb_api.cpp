@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -48,6 +49,16 @@ std::atomic<int64_t> g_launches{0};
 void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 thread_local cudaStream_t tl_user_stream = nullptr;
+
+// FP32 guard-band search (k_search2.cu) on/off; NLB_FP64_SEARCH=1 selects the
+// all-FP64 kernels (same results) for comparisons.
+bool fp32_search_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("NLB_FP64_SEARCH");
+    return !(v && v[0] == '1');
+  }();
+  return on;
+}
 thread_local bool tl_profile = false;
 
 // ------------------------------------------------------------------ pinned pool
@@ -196,20 +207,33 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
   const int64_t n = sp.n;
   const int32_t k = (int32_t)sp.rc_sq.size();
   cudaStream_t s = c.stream;
-  sp.counts = slot<uint32_t>(c, kSlotCounts, (size_t)k * (n + 1));
-  sp.offs = slot<int64_t>(c, kSlotOffs, (size_t)k * (n + 1) + 1);
-  int64_t* scan_tmp =
-      slot<int64_t>(c, kSlotScanTmp, (size_t)scan_tmp_elems(std::max<int64_t>(
-                                          (int64_t)k * (n + 1), sp.grid.total_bins)));
+  // Count layout: k rows of n + 1 per-atom counts, or (pair tasks) one row of
+  // n * S per-(atom, stencil cell) counts plus a trailing zero.
+  const int64_t cells = sp.fp32 ? (int64_t)(2 * sp.grid.ns[0] + 1) * (2 * sp.grid.ns[1] + 1) *
+                                      (2 * sp.grid.ns[2] + 1)
+                                : 0;
+  const int64_t row = sp.fp32 ? n * cells + 1 : n + 1;
+  sp.row = row;
+  sp.counts = slot<uint32_t>(c, kSlotCounts, (size_t)k * row);
+  sp.offs = slot<int64_t>(c, kSlotOffs, (size_t)k * row + 1);
+  int64_t* scan_tmp = slot<int64_t>(
+      c, kSlotScanTmp, (size_t)scan_tmp_elems(std::max<int64_t>((int64_t)k * row, sp.grid.total_bins)));
   if (!sp.counts || !sp.offs || !scan_tmp) return fail(NLB_ERR_NOMEM, "device allocation failed");
 
   c.mark(0);
   if (sp.method == Method::kCellList) {
     GridBuffers& b = sp.gb;
     const int64_t nb = sp.grid.total_bins;
+    const size_t tab_cap_before = c.bufs[kSlotRankTab].cap;
+    const void* tab_before = c.bufs[kSlotRankTab].p;
     b.rank_of_bin = slot<int32_t>(c, kSlotRankTab, nb);
-    b.bin_count = slot<int32_t>(c, kSlotBinCount, nb);
-    b.bin_fill = slot<int32_t>(c, kSlotBinFill, nb);
+    const bool same_tab = b.rank_of_bin == tab_before && tab_cap_before > 0 &&
+                          c.rank_nb[0] == sp.grid.nb[0] && c.rank_nb[1] == sp.grid.nb[1] &&
+                          c.rank_nb[2] == sp.grid.nb[2];
+    // One zeroed block: bin histogram, scatter cursors, pair-task counters.
+    int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 2);
+    b.bin_count = zeroed;
+    b.bin_fill = zeroed ? zeroed + nb : nullptr;
     b.bin_start = slot<int64_t>(c, kSlotBinStart, nb + 1);
     b.key = slot<uint64_t>(c, kSlotKey, n);
     b.rank = slot<int32_t>(c, kSlotRank, n);
@@ -222,32 +246,54 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
     b.pz = slot<double>(c, kSlotPz, n);
     b.meta = slot<SlotMeta>(c, kSlotMeta, n);
     b.scan_tmp = scan_tmp;
+    b.p32 = nullptr;
+    b.sbin = nullptr;
+    b.groups = nullptr;
+    b.irr_list = nullptr;
+    b.irr = nullptr;
+    b.counters = nullptr;
+    if (sp.fp32) {
+      b.p32 = slot<float4>(c, kSlotP32, n);
+      b.sbin = slot<int32_t>(c, kSlotSbin, n);
+      b.groups = slot<int2>(c, kSlotGroups, n / 32 + std::min<int64_t>(n, nb) + 1);
+      b.irr_list = slot<int32_t>(c, kSlotIrrList, n);
+      b.irr = slot<uint8_t>(c, kSlotIrr, n);
+      b.counters = zeroed ? zeroed + 2 * nb : nullptr;
+      if (!b.p32 || !b.sbin || !b.groups || !b.irr_list || !b.irr || !b.counters)
+        return fail(NLB_ERR_NOMEM, "device allocation failed");
+    }
     if (!b.rank_of_bin || !b.bin_count || !b.bin_fill || !b.bin_start || !b.key || !b.rank ||
         !b.skey || !b.sidx || !b.skey2 || !b.sidx2 || !b.px || !b.py || !b.pz || !b.meta)
       return fail(NLB_ERR_NOMEM, "device allocation failed");
-    cudaMemsetAsync(b.bin_count, 0, sizeof(int32_t) * nb, s);
-    cudaMemsetAsync(b.bin_fill, 0, sizeof(int32_t) * nb, s);
-    launch_grid_build(sp.grid, d_pos, n, b, s);
+    cudaMemsetAsync(zeroed, 0, sizeof(int32_t) * (2 * (size_t)nb + 2), s);
+    launch_grid_build(sp.grid, d_pos, n, b, s, !same_tab);
+    for (int a = 0; a < 3; ++a) c.rank_nb[a] = sp.grid.nb[a];
   }
   c.mark(1);
   for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
     CutoffSet cs = sp.pass(g0);
-    uint32_t* rows = sp.counts + (size_t)g0 * (n + 1);
-    if (sp.method == Method::kCellList)
+    uint32_t* rows = sp.counts + (size_t)g0 * row;
+    if (sp.method == Method::kCellList && sp.fp32)
+      launch_pair_count(sp.grid, sp.gb, n, sp.band, rows, s);
+    else if (sp.method == Method::kCellList)
       launch_grid_count(sp.grid, sp.gb, n, cs, rows, s);
     else
       launch_brute_count(sp.brute, d_pos, n, cs, rows, s);
   }
   c.mark(2);
-  exclusive_scan_u32(sp.counts, (int64_t)k * (n + 1), sp.offs, scan_tmp, s);
+  exclusive_scan_u32(sp.counts, (int64_t)k * row, sp.offs, scan_tmp, s);
   c.mark(3);
-  // Row starts offs[q * (n + 1)], q = 0..k, in one strided copy.
+  // Row starts offs[q * row], q = 0..k, in one strided copy.
   if (k + 1 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
-  cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), sp.offs, sizeof(int64_t) * (n + 1),
+  cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), sp.offs, sizeof(int64_t) * row,
                                     sizeof(int64_t), (size_t)k + 1, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)  // the scan's bounded-wait error word
+    e = cudaMemcpyAsync(c.h_small + k + 1, scan_tmp + 1, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                        s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy2DAsync");
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "count pass");
+  if (c.h_small[k + 1] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
   if (c.prof) {
     c.harvest();  // a previous emit on this stream is complete too
     c.prof_pending_count = true;
@@ -274,8 +320,10 @@ Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& 
       t.base[q] = base[g0 + q];
     }
     t.index_offset = index_offset;
-    const int64_t* offs = sp.offs + (size_t)g0 * (sp.n + 1);
-    if (sp.method == Method::kCellList)
+    const int64_t* offs = sp.offs + (size_t)g0 * sp.row;
+    if (sp.method == Method::kCellList && sp.fp32)
+      launch_pair_emit(sp.grid, sp.gb, sp.n, sp.band, offs, t, c.stream);
+    else if (sp.method == Method::kCellList)
       launch_grid_emit(sp.grid, sp.gb, sp.n, cs, offs, t, c.stream);
     else
       launch_brute_emit(sp.brute, d_pos, sp.n, cs, offs, t, c.stream);
@@ -331,6 +379,7 @@ Status plan_system(const double* pos_host, int64_t n, const double* cell9, const
     for (int a = 0; a < 3; ++a)
       if (sp.grid.ns[a] < 0 || sp.grid.ns[a] > (1 << 20))
         return fail(NLB_ERR_VALUE, "stencil too large for this cutoff and cell");
+    sp.fp32 = k == 1 && fp32_search_enabled() && make_guard_band(sp.grid, rc_max, sp.band);
   } else {
     std::memcpy(sp.brute.h, sp.cell.h, sizeof(sp.brute.h));
     std::memcpy(sp.brute.hinv, sp.cell.hinv, sizeof(sp.brute.hinv));

@@ -125,13 +125,17 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
   c.mark(2);
   exclusive_scan_u32(counts, (int64_t)k * row, offs, scan_tmp, s);
   c.mark(3);
-  if (k + 2 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
+  if (k + 3 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
   cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), offs, sizeof(int64_t) * row,
                                     sizeof(int64_t), (size_t)k + 1, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(c.h_small + k + 1, flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)  // the scan's bounded-wait error word
+    e = cudaMemcpyAsync(c.h_small + k + 2, scan_tmp + 1, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                        s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "batched count pass");
+  if (c.h_small[k + 2] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
   if (c.prof) {
     c.harvest();
     c.prof_pending_count = true;

@@ -27,6 +27,7 @@ struct GridParams {
   double origin[3];    // H (0.5/nb)
   double prune_sq;     // (sqrt(rc_max^2) + bin_bounding_radius)^2
   int64_t total_bins;
+  double radius;       // bin bounding radius (half the largest bin diagonal)
 };
 
 // Sorted-slot payload that travels with a candidate: wrap shift and the

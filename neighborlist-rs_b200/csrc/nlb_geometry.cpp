@@ -158,6 +158,7 @@ void plan_grid(const HostCell& c, double rc, GridParams& g) {
   const double mx =
       fmax_nan_ignoring(fmax_nan_ignoring(fmax_nan_ignoring(d[0], d[1]), d[2]), d[3]);
   const double radius = 0.5 * std::sqrt(mx);
+  g.radius = radius;
   // prune_limit = sqrt(rc*rc) + R (src/search.rs:488-489): the square root of
   // the squared cutoff is taken, not rc itself.
   const double pl = std::sqrt(rc * rc) + radius;

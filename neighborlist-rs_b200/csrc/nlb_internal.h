@@ -44,6 +44,12 @@ enum Slot : int {
   kSlotOffs,
   kSlotOutEi,
   kSlotOutSh,
+  kSlotP32,
+  kSlotSbin,
+  kSlotGroups,
+  kSlotIrrList,
+  kSlotIrr,
+  kSlotCounters,
   kSlotBatch0,  // first slot owned by the batched path
   kSlotCount = kSlotBatch0 + 32,
 };
@@ -67,6 +73,8 @@ struct Ctx {
   bool prof_pending_emit = false;
   cudaEvent_t ev[6] = {};
   double prof_ms[4] = {0, 0, 0, 0};
+  // Bins per axis of the rank table currently in kSlotRankTab (-1: none).
+  int32_t rank_nb[3] = {-1, -1, -1};
   int64_t prof_calls = 0;
   void mark(int i) {
     if (prof) cudaEventRecord(ev[i], stream);
@@ -78,6 +86,7 @@ struct Ctx {
 };
 
 Status get_ctx(Ctx** out);
+bool fp32_search_enabled();
 
 template <class T>
 inline T* slot(Ctx& c, int s, size_t count) {
@@ -101,8 +110,11 @@ struct SystemPlan {
   std::vector<int32_t> order;   // sorted position q -> input cutoff index
   std::vector<double> rc_sq;    // ascending squared cutoffs
   std::vector<int64_t> m;       // edges per sorted cutoff (after count)
+  bool fp32 = false;            // single cutoff, cell list: FP32 guard-band kernels
+  GuardBand band{};
   uint32_t* counts = nullptr;
   int64_t* offs = nullptr;
+  int64_t row = 0;              // length of one cutoff's count row
   CutoffSet pass(int32_t g0) const;
 };
 

@@ -35,10 +35,27 @@ struct GridBuffers {
   double* pz;
   SlotMeta* meta;         // [n] sorted wrap shifts + original index
   int64_t* scan_tmp;
+  // Optional (nullptr = not produced): FP32 position of each sorted atom
+  // relative to its own bin centre, with the original index in .w, and the
+  // atom's linear bin index.  Used by the FP32 guard-band search kernels.
+  float4* p32;
+  int32_t* sbin;
+  // Work lists for the pair-task search (k_search2.cu), filled by the build
+  // when p32 is set: groups[g] = {first sorted slot, bin rank} of each run of
+  // at most 32 atoms of one bin; irr_list = sorted slots of atoms whose home
+  // stencil (recomputed from the wrapped position) differs from their stored
+  // bin; irr[p] = 1 for those atoms; counters[0] = #groups, [1] = #irregular
+  // (zeroed by the caller before the build).
+  int2* groups;
+  int32_t* irr_list;
+  uint8_t* irr;
+  int32_t* counters;
 };
 
+// need_rank_table = false reuses rank_of_bin from a previous build with the
+// same bins per axis.
 void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const GridBuffers& b,
-                       cudaStream_t s);
+                       cudaStream_t s, bool need_rank_table = true);
 
 // ---- k_search.cu : count / emit (src/search.rs:291-446, :448-1078, :1187-1405)
 struct CutoffSet {
@@ -62,6 +79,29 @@ void launch_grid_count(const GridParams& g, const GridBuffers& b, int64_t n,
                        const CutoffSet& cs, uint32_t* counts, cudaStream_t s);
 void launch_grid_emit(const GridParams& g, const GridBuffers& b, int64_t n, const CutoffSet& cs,
                       const int64_t* offs, const EmitTargets& t, cudaStream_t s);
+
+// ---- k_search2.cu : single-cutoff search as (atom group, stencil cell)
+// tasks with an FP32 pair test and an exact FP64 recheck inside a guard band
+// around rc^2 (see k_search2.cu).
+struct GuardBand {
+  float lo;       // d2_32 < lo  => certainly inside (d2_64 < rc^2)
+  float hi;       // d2_32 >= hi => certainly outside
+  double rc_sq;   // exact test for d2_32 in [lo, hi)
+};
+// Stencils above this many cells use the per-atom FP64 kernels.
+constexpr int64_t kPairMaxCells = 1024;
+// Returns false when the FP32 test cannot be made safe for this grid (the
+// band would be too wide); callers then use the FP64 kernels.
+bool make_guard_band(const GridParams& g, double rc, GuardBand& band);
+// counts[p * S + c] (S = stencil cells) for every sorted atom p and cell c,
+// plus counts[n * S] = 0.
+void launch_pair_count(const GridParams& g, const GridBuffers& b, int64_t n,
+                       const GuardBand& band, uint32_t* counts, cudaStream_t s);
+// offs = exclusive scan of those counts; edges of (p, c) start at
+// t.base[0] + offs[p * S + c] - offs[0].
+void launch_pair_emit(const GridParams& g, const GridBuffers& b, int64_t n,
+                      const GuardBand& band, const int64_t* offs, const EmitTargets& t,
+                      cudaStream_t s);
 
 enum BruteMode : int32_t { kBruteRaw = 0, kBruteMicMode = 1 };
 struct BruteParams {

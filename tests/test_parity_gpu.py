@@ -265,3 +265,30 @@ def test_batch_thresholds_and_self_images(nl, oracle):
         finally:
             nl.set_brute_force_threshold(1000)
             oracle.set_thresholds(1000, 300)
+
+
+@pytest.mark.parametrize("jitter", [0.0, 1e-9, 1e-6])
+def test_guard_band_near_cutoff(nl, oracle, jitter):
+    """Lattice pairs exactly at (or within 1e-9 / 1e-6 A of) the cutoff: the
+    FP32 test must defer every undecidable pair to the exact FP64 expression."""
+    a = 2.0
+    g = np.arange(10) * a
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pos = pos + np.random.default_rng(3).normal(0.0, jitter, pos.shape) if jitter else pos
+    for rc in (2.0, np.sqrt(8.0), np.sqrt(12.0), 4.0, 2.0 * np.nextafter(1.0, 2.0)):
+        single(nl, oracle, pos, eye(20.0), float(rc), what=f"lattice rc={rc!r} jitter={jitter}")
+        single(nl, oracle, pos + 0.5, eye(20.0), float(rc), what=f"lattice+0.5 rc={rc!r}")
+    tri = np.array([[20.0, 3.0, 1.0], [0.0, 20.0, 2.0], [0.0, 0.0, 20.0]])
+    single(nl, oracle, pos @ tri.T / 20.0, tri, 2.0 * 1.0000001, what="skewed lattice")
+
+
+def test_large_system_many_scan_tiles(nl, oracle):
+    """200k atoms at density 0.1 (5.4 M per-(atom, cell) counts: ~1300 tiles of
+    the single-pass scan), plus grid-shape changes between calls."""
+    rng = np.random.default_rng(77)
+    L = (200_000 / 0.1) ** (1 / 3)
+    pos = rng.random((200_000, 3)) * L
+    single(nl, oracle, pos, eye(L), 5.0, what="200k atoms rc 5")
+    small = pos[:20_000] * 0.5
+    for rc in (6.0, 3.0, 6.0):
+        single(nl, oracle, small, eye(L * 0.5), rc, what=f"grid change rc {rc}")
