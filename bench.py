@@ -363,6 +363,22 @@ def run_b200(args):
     barrier(world)
 
 
+def median_call(fn, reps=5, warmup=2):
+    """Median wall time of fn() over reps calls (results released between
+    calls so pinned result buffers are reused); returns (seconds, result)."""
+    for _ in range(warmup):
+        r = fn()
+        del r
+    ts = []
+    r = None
+    for _ in range(reps):
+        r = None
+        t0 = time.perf_counter()
+        r = fn()
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts), r
+
+
 def extra_measurements(nl, torch, args):
     from neighborlist_rs import workloads as W
 
@@ -382,26 +398,30 @@ def extra_measurements(nl, torch, args):
     # triclinic multi-cutoff (host-buffer call)
     p3, r3 = W.triclinic_uniform()
     cell = nl.PyCell(r3.T.tolist())
-    nl.build_neighborlists_multi(cell, p3, [5.0, 6.0, 12.0])
-    t0 = time.perf_counter()
-    reps = 3
-    for _ in range(reps):
-        r = nl.build_neighborlists_multi(cell, p3, [5.0, 6.0, 12.0])
-    dtm = (time.perf_counter() - t0) / reps
+    t3, r = median_call(lambda: nl.build_neighborlists_multi(cell, p3, [5.0, 6.0, 12.0]))
     m3 = sum(v["edge_index"].shape[1] for v in r.values())
-    out["triclinic_multi_e2e"] = {"edges_per_s": m3 / dtm, "ms_per_call": 1e3 * dtm,
-                                  "edges": m3}
-    # batched uneven systems (host-buffer call)
+    del r
+    out["triclinic_multi_e2e"] = {"edges_per_s": m3 / t3, "ms_per_call": 1e3 * t3, "edges": m3}
+    # batched uneven systems (host-buffer call) vs the plain per-system loop
     systems = W.uneven_batch()
     pb, bb, cb = W.concat_batch(systems)
-    nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0)
-    t0 = time.perf_counter()
-    rb = nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0)
-    dtb = time.perf_counter() - t0
-    out["uneven_batch_4096_e2e"] = {"systems_per_s": len(systems) / dtb,
-                                    "edges_per_s": rb["edge_index"].shape[1] / dtb,
-                                    "ms_per_call": 1e3 * dtb, "atoms": int(pb.shape[0]),
-                                    "edges": int(rb["edge_index"].shape[1])}
+    nl.profile(True)
+    tb, rb = median_call(lambda: nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0))
+    calls, ph = nl.profile_read()
+    nl.profile(False)
+    mb = int(rb["edge_index"].shape[1])
+    del rb
+    dev_ms = sum(ph.values()) / max(calls, 1)
+    cells = [None if s.cell_rows is None else nl.PyCell(s.cell_rows.T.tolist()) for s in systems]
+    sample = 512
+    tp, _ = median_call(lambda: [nl.build_neighborlists(cells[i], systems[i].positions, 5.0)
+                                 for i in range(sample)], reps=3, warmup=1)
+    out["uneven_batch_4096"] = {
+        "systems_per_s_e2e": len(systems) / tb, "edges_per_s_e2e": mb / tb,
+        "ms_per_call_e2e": 1e3 * tb, "systems_per_s_device": len(systems) / (dev_ms * 1e-3),
+        "device_ms_phases": {k: v / max(calls, 1) for k, v in ph.items()},
+        "plain_per_system_loop_systems_per_s": sample / tp,
+        "atoms": int(pb.shape[0]), "edges": mb}
     return out
 
 

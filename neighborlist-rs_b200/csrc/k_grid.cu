@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kSortThreads)
               uint64_t* __restrict__ skey2, int32_t* __restrict__ sidx2,
               double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz,
               SlotMeta* __restrict__ meta, float4* __restrict__ p32, int32_t* __restrict__ sbin,
-              int2* __restrict__ groups, int32_t* __restrict__ irr_list,
+              GroupRec* __restrict__ groups, int32_t* __restrict__ irr_list,
               uint8_t* __restrict__ irr, int32_t* __restrict__ counters) {
   __shared__ uint64_t sk[kSortCap];
   __shared__ int32_t sv[kSortCap];
@@ -242,7 +242,17 @@ __global__ void __launch_bounds__(kSortThreads)
   if (p32 && threadIdx.x == 0) {
     const int ng = (int)((cnt + 31) / 32);
     const int base = atomicAdd(&counters[0], ng);
-    for (int k = 0; k < ng; ++k) groups[base + k] = make_int2((int)(s + 32 * k), (int)r);
+    const int32_t lin = sbin[s];
+    GroupRec gr;
+    gr.end = (int32_t)e;
+    gr.lin = lin;
+    gr.bx = lin % g.nb[0];
+    gr.by = (lin / g.nb[0]) % g.nb[1];
+    gr.bz = lin / (g.nb[0] * g.nb[1]);
+    for (int k = 0; k < ng; ++k) {
+      gr.first = (int32_t)(s + 32 * k);
+      groups[base + k] = gr;
+    }
   }
 }
 

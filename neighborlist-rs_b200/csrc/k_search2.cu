@@ -85,7 +85,7 @@ template <bool EMIT>
 __device__ void pair_irregular(const GridParams& g, const GridBuffers& b, int32_t n_cells,
                                double rc_sq, uint32_t* __restrict__ counts,
                                const int64_t* __restrict__ offs, const EmitTargets& t,
-                               int64_t gwarp, int64_t nwarps) {
+                               int64_t* __restrict__ dst0, int64_t gwarp, int64_t nwarps) {
   const int lane = threadIdx.x & 31;
   const int32_t n_irr = b.counters[1];
   const int64_t off0 = EMIT ? offs[0] : 0;
@@ -128,7 +128,7 @@ __device__ void pair_irregular(const GridParams& g, const GridBuffers& b, int32_
             if (hit) {
               const int64_t e = slot + __popc(m & lanemask_lt());
               t.src[0][e] = (int64_t)mi.orig + t.index_offset;
-              t.dst[0][e] = (int64_t)jo + t.index_offset;
+              dst0[e] = (int64_t)jo + t.index_offset;
               int32_t* sp = t.sh[0] + 3 * e;
               sp[0] = (mj.sx - mi.sx) + d.sh[0];
               sp[1] = (mj.sy - mi.sy) + d.sh[1];
@@ -143,87 +143,150 @@ __device__ void pair_irregular(const GridParams& g, const GridBuffers& b, int32_
   }
 }
 
+// Euclidean division with the common in-range cases first.
+__device__ __forceinline__ void div_mod_fast(int32_t v, int32_t m, int32_t& rem, int32_t& quot) {
+  if (v >= 0 && v < m) {
+    rem = v;
+    quot = 0;
+  } else if (v < 0 && v >= -m) {
+    rem = v + m;
+    quot = -1;
+  } else if (v >= m && v < 2 * m) {
+    rem = v - m;
+    quot = 1;
+  } else {
+    div_mod(v, m, rem, quot);
+  }
+}
+
 template <bool EMIT>
 __global__ void __launch_bounds__(kPairWarps * 32)
     k_pair_tasks(GridParams g, GridBuffers b, int64_t n, int32_t n_cells, GuardBand band,
                  uint32_t* __restrict__ counts, const int64_t* __restrict__ offs, EmitTargets t) {
   __shared__ float4 stage_q[kPairWarps][32];
   __shared__ SlotMeta stage_m[kPairWarps][32];
+  __shared__ char4 stencil[kPairMaxCells];  // (dx, dy, dz) of each stencil cell, x outer
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  {
+    const int32_t ny = 2 * g.ns[1] + 1, nz = 2 * g.ns[2] + 1;
+    for (int c = threadIdx.x; c < n_cells; c += blockDim.x) {
+      const int32_t ix = c / (ny * nz);
+      const int32_t rem = c - ix * (ny * nz);
+      const int32_t iy = rem / nz;
+      stencil[c] = make_char4((signed char)(ix - g.ns[0]), (signed char)(iy - g.ns[1]),
+                              (signed char)(rem - iy * nz - g.ns[2]), 0);
+    }
+    __syncthreads();
+  }
   float4* sq = stage_q[warp];
   SlotMeta* smt = stage_m[warp];
-  const int64_t n_tasks = (int64_t)b.counters[0] * n_cells;
-  const int64_t step = (int64_t)gridDim.x * kPairWarps;
+  int64_t* dst0 = EMIT ? t.dst[0] : nullptr;
+  if (EMIT && t.total_dev) {
+    const int64_t m_total = *t.total_dev;
+    if (m_total > t.capacity) return;  // the caller grows the arena and emits again
+    dst0 = t.src[0] + m_total;
+  }
+  const uint32_t n_tasks = (uint32_t)b.counters[0] * (uint32_t)n_cells;
+  const uint32_t step = gridDim.x * kPairWarps;
   const int64_t off0 = EMIT ? offs[0] : 0;
+  const float lo = band.lo, hi = band.hi;
 
-  for (int64_t task = (int64_t)blockIdx.x * kPairWarps + warp; task < n_tasks; task += step) {
-    const int32_t gi = (int32_t)(task / n_cells);
-    const int32_t c = (int32_t)(task - (int64_t)gi * n_cells);
-    const int2 grp = b.groups[gi];
-    const int32_t first = grp.x;
-    const int32_t bin_end = (int32_t)b.bin_start[grp.y + 1];
-    const int32_t len = bin_end - first < 32 ? bin_end - first : 32;
-    const int32_t p = first + (lane < len ? lane : 0);
+  for (uint32_t task = blockIdx.x * kPairWarps + warp; task < n_tasks; task += step) {
+    const uint32_t gi = task / (uint32_t)n_cells;
+    const int32_t c = (int32_t)(task - gi * (uint32_t)n_cells);
+    const GroupRec grp = b.groups[gi];
+    const int32_t len = grp.end - grp.first < 32 ? grp.end - grp.first : 32;
+    const int32_t p = grp.first + (lane < len ? lane : 0);
     const bool mine = lane < len && !b.irr[p];
 
-    // The group's bin (stored and home stencil centre for regular atoms).
-    const int32_t lin = b.sbin[first];
-    int32_t home[3];
-    home[0] = lin % g.nb[0];
-    home[1] = (lin / g.nb[0]) % g.nb[1];
-    home[2] = lin / (g.nb[0] * g.nb[1]);
-    const CellDesc d = describe_cell(g, b, home, c);
-    double cb[3];
-    bin_centre(g, lin, cb);
+    // The stencil cell (shared by the group) and the group's bin centre.
+    const char4 st = stencil[c];
+    int32_t bin[3], sh[3];
+    div_mod_fast(grp.bx + st.x, g.nb[0], bin[0], sh[0]);
+    div_mod_fast(grp.by + st.y, g.nb[1], bin[1], sh[1]);
+    div_mod_fast(grp.bz + st.z, g.nb[2], bin[2], sh[2]);
+    double off[3], cs[3], cb[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      off[k] = dadd(dadd(dmul(g.h[3 * k], (double)sh[0]), dmul(g.h[3 * k + 1], (double)sh[1])),
+                    dmul(g.h[3 * k + 2], (double)sh[2]));
+      double v = dadd(g.origin[k], dmul(g.basis[0][k], (double)bin[0]));
+      v = dadd(v, dmul(g.basis[1][k], (double)bin[1]));
+      v = dadd(v, dmul(g.basis[2][k], (double)bin[2]));
+      cs[k] = dadd(v, off[k]);
+      double w = dadd(g.origin[k], dmul(g.basis[0][k], (double)grp.bx));
+      w = dadd(w, dmul(g.basis[1][k], (double)grp.by));
+      cb[k] = dadd(w, dmul(g.basis[2][k], (double)grp.bz));
+    }
+    const int64_t lin = bin[0] + (int64_t)g.nb[0] * (bin[1] + (int64_t)g.nb[1] * bin[2]);
+    const int32_t r = b.rank_of_bin[lin];
+    const int32_t b0 = (int32_t)b.bin_start[r], b1 = (int32_t)b.bin_start[r + 1];
 
     const double xi = b.px[p], yi = b.py[p], zi = b.pz[p];
     const bool live =
-        mine && !(norm2(dsub(d.cs[0], xi), dsub(d.cs[1], yi), dsub(d.cs[2], zi)) > g.prune_sq);
+        mine && !(norm2(dsub(cs[0], xi), dsub(cs[1], yi), dsub(cs[2], zi)) > g.prune_sq);
     uint32_t cnt = 0;
     int64_t slot = 0;
     if (EMIT && mine) slot = t.base[0] + (offs[(int64_t)p * n_cells + c] - off0);
-    if (__any_sync(0xffffffffu, live) && d.b1 > d.b0) {
+    if (__any_sync(0xffffffffu, live) && b1 > b0) {
       const float4 a = b.p32[p];
       const int32_t io = __float_as_int(a.w);
-      const float ux = __double2float_rn(dsub(d.cs[0], cb[0])) - a.x;
-      const float uy = __double2float_rn(dsub(d.cs[1], cb[1])) - a.y;
-      const float uz = __double2float_rn(dsub(d.cs[2], cb[2])) - a.z;
-      const bool shifted = (d.sh[0] | d.sh[1] | d.sh[2]) != 0;
+      const float ux = __double2float_rn(dsub(cs[0], cb[0])) - a.x;
+      const float uy = __double2float_rn(dsub(cs[1], cb[1])) - a.y;
+      const float uz = __double2float_rn(dsub(cs[2], cb[2])) - a.z;
+      const bool shifted = (sh[0] | sh[1] | sh[2]) != 0;
       SlotMeta mi;
       if (EMIT) mi = b.meta[p];
-      for (int32_t jb = d.b0; jb < d.b1; jb += 32) {
-        const int32_t nj = d.b1 - jb < 32 ? d.b1 - jb : 32;
+      for (int32_t jb = b0; jb < b1; jb += 32) {
+        const int32_t nj = b1 - jb < 32 ? b1 - jb : 32;
+        // Stage 32 candidates; slots past the bin end hold a far sentinel.
+        float4 qv = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
         if (lane < nj) {
-          sq[lane] = b.p32[jb + lane];
+          qv = b.p32[jb + lane];
           if (EMIT) smt[lane] = b.meta[jb + lane];
         }
+        sq[lane] = qv;
         __syncwarp();
-        for (int32_t jj = 0; jj < nj; ++jj) {
+        // FP32 test of all 32 staged candidates into bit masks.
+        uint32_t inside = 0, maybe = 0, order = 0;
+#pragma unroll
+        for (int jj = 0; jj < 32; ++jj) {
           const float4 q = sq[jj];
           const float dx = q.x + ux;
           const float dy = q.y + uy;
           const float dz = q.z + uz;
           const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
-          bool in = d2 < band.lo;
-          if (live && !in && d2 < band.hi) {
-            const int32_t j = jb + jj;
-            const double ex = dadd(dsub(b.px[j], xi), d.off[0]);
-            const double ey = dadd(dsub(b.py[j], yi), d.off[1]);
-            const double ez = dadd(dsub(b.pz[j], zi), d.off[2]);
-            in = norm2(ex, ey, ez) < band.rc_sq;
-          }
           const int32_t jo = __float_as_int(q.w);
-          const bool hit = live && in && (io < jo || (io == jo && shifted));
-          if (!EMIT) {
-            cnt += hit ? 1u : 0u;
-          } else if (hit) {
+          inside |= (uint32_t)(d2 < lo) << jj;
+          maybe |= (uint32_t)(d2 < hi) << jj;
+          order |= (uint32_t)(io < jo || (io == jo && shifted)) << jj;
+        }
+        if (!live) order = 0;
+        // Guard band: the reference's exact FP64 test decides.
+        uint32_t amb = maybe & ~inside & order;
+        while (amb) {
+          const int jj = __ffs(amb) - 1;
+          amb &= amb - 1;
+          const int32_t j = jb + jj;
+          const double ex = dadd(dsub(b.px[j], xi), off[0]);
+          const double ey = dadd(dsub(b.py[j], yi), off[1]);
+          const double ez = dadd(dsub(b.pz[j], zi), off[2]);
+          if (norm2(ex, ey, ez) < band.rc_sq) inside |= 1u << jj;
+        }
+        uint32_t hits = inside & order;
+        if (!EMIT) {
+          cnt += __popc(hits);
+        } else {
+          while (hits) {
+            const int jj = __ffs(hits) - 1;
+            hits &= hits - 1;
             const SlotMeta mj = smt[jj];
             t.src[0][slot] = (int64_t)io + t.index_offset;
-            t.dst[0][slot] = (int64_t)jo + t.index_offset;
+            dst0[slot] = (int64_t)mj.orig + t.index_offset;
             int32_t* sp = t.sh[0] + 3 * slot;
-            sp[0] = (mj.sx - mi.sx) + d.sh[0];
-            sp[1] = (mj.sy - mi.sy) + d.sh[1];
-            sp[2] = (mj.sz - mi.sz) + d.sh[2];
+            sp[0] = (mj.sx - mi.sx) + sh[0];
+            sp[1] = (mj.sy - mi.sy) + sh[1];
+            sp[2] = (mj.sz - mi.sz) + sh[2];
             ++slot;
           }
         }
@@ -233,7 +296,7 @@ __global__ void __launch_bounds__(kPairWarps * 32)
     if (!EMIT && mine) counts[(int64_t)p * n_cells + c] = cnt;
   }
   // Atoms whose home stencil is not their stored bin (normally none).
-  pair_irregular<EMIT>(g, b, n_cells, band.rc_sq, counts, offs, t,
+  pair_irregular<EMIT>(g, b, n_cells, band.rc_sq, counts, offs, t, dst0,
                        (int64_t)blockIdx.x * kPairWarps + warp, step);
   if (!EMIT && blockIdx.x == 0 && threadIdx.x == 0) counts[n * (int64_t)n_cells] = 0;
 }

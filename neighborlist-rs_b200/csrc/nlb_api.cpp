@@ -255,7 +255,7 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
     if (sp.fp32) {
       b.p32 = slot<float4>(c, kSlotP32, n);
       b.sbin = slot<int32_t>(c, kSlotSbin, n);
-      b.groups = slot<int2>(c, kSlotGroups, n / 32 + std::min<int64_t>(n, nb) + 1);
+      b.groups = slot<GroupRec>(c, kSlotGroups, n / 32 + std::min<int64_t>(n, nb) + 1);
       b.irr_list = slot<int32_t>(c, kSlotIrrList, n);
       b.irr = slot<uint8_t>(c, kSlotIrr, n);
       b.counters = zeroed ? zeroed + 2 * nb : nullptr;
@@ -504,6 +504,18 @@ Status run_single(const double* pos, int64_t n, const double* cell9, const uint8
   double* d_pos = nullptr;
   st = upload_positions(*c, pos, n, &d_pos);
   if (!st.ok()) return st;
+  if (fast_eligible(sp)) {
+    int64_t m = 0;
+    st = run_fast(*c, sp, d_pos, &m);
+    if (!st.ok()) return st;
+    DevLists L;
+    L.src.assign(1, sp.out_src);
+    L.dst.assign(1, sp.out_src + m);
+    L.sh.assign(1, sp.out_sh);
+    st = download_results(*c, std::vector<int64_t>(1, m), L, sp.order, outs);
+    if (!st.ok()) nlb_result_free(&outs[0]);
+    return st;
+  }
   st = count_system(*c, sp, d_pos);
   if (!st.ok()) return st;
   DevLists L;
@@ -549,6 +561,15 @@ Status run_single_device(const double* d_pos, int64_t n, const double* cell9, co
   std::vector<double> cs(1, cutoff);
   st = plan_system(nullptr, n, cell9, pb, cs, false, false, sp, bptr);
   if (!st.ok()) return st;
+  if (fast_eligible(sp)) {
+    int64_t m = 0;
+    st = run_fast(*c, sp, d_pos, &m);
+    if (!st.ok()) return st;
+    out->n_edges = m;
+    out->edge_index = sp.out_src;
+    out->shift = sp.out_sh;
+    return Status{NLB_OK};
+  }
   st = count_system(*c, sp, d_pos);
   if (!st.ok()) return st;
   DevLists L;

@@ -30,6 +30,13 @@ struct GridParams {
   double radius;       // bin bounding radius (half the largest bin diagonal)
 };
 
+// A run of at most 32 atoms of one bin (a pair-task group).
+struct alignas(8) GroupRec {
+  int32_t first, end;  // sorted slots [first, min(first + 32, end)); end = bin end
+  int32_t bx, by, bz;  // the bin's coordinates
+  int32_t lin;         // its linear index
+};
+
 // Sorted-slot payload that travels with a candidate: wrap shift and the
 // original atom index, loaded as one 16-byte vector.
 struct alignas(16) SlotMeta {

@@ -115,6 +115,9 @@ struct SystemPlan {
   uint32_t* counts = nullptr;
   int64_t* offs = nullptr;
   int64_t row = 0;              // length of one cutoff's count row
+  bool rank_cached = false;     // fast path: rank table reusable
+  int64_t* out_src = nullptr;   // fast path: [src | dst] arena
+  int32_t* out_sh = nullptr;    // fast path: shift arena
   CutoffSet pass(int32_t g0) const;
 };
 
@@ -132,6 +135,15 @@ Status plan_system(const double* pos_host, int64_t n, const double* cell9, const
 Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos);
 Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& L,
                    const int64_t* base, int64_t index_offset);
+
+// Single-cutoff cell-list pipeline with one synchronisation, replayed as a
+// CUDA graph for repeated identical calls (nlb_fast.cpp).  Requires
+// sp.method == kCellList and sp.fp32; leaves the M edges in sp.out_src
+// ([src | dst]) and sp.out_sh.
+Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out);
+inline bool fast_eligible(const SystemPlan& sp) {
+  return sp.method == Method::kCellList && sp.fp32 && sp.rc_sq.size() == 1;
+}
 
 Status alloc_result(int64_t m, nlb_result* r);
 void zero_results(nlb_result* outs, int32_t k);

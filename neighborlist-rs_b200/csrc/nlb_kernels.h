@@ -46,7 +46,7 @@ struct GridBuffers {
   // stencil (recomputed from the wrapped position) differs from their stored
   // bin; irr[p] = 1 for those atoms; counters[0] = #groups, [1] = #irregular
   // (zeroed by the caller before the build).
-  int2* groups;
+  GroupRec* groups;
   int32_t* irr_list;
   uint8_t* irr;
   int32_t* counters;
@@ -72,6 +72,11 @@ struct EmitTargets {
   int32_t* sh[kMaxCutoffsPerPass];   // shifts per cutoff: [3e .. 3e+2]
   int64_t base[kMaxCutoffsPerPass];  // first edge slot of this system per cutoff
   int64_t index_offset;              // added to both atom indices (batched systems)
+  // Pair-task emit only: when set, the list's total M is read from device
+  // memory, destinations go to src[0] + M (the [src | dst] layout), and
+  // nothing is written if M > capacity (the caller grows and re-emits).
+  const int64_t* total_dev;
+  int64_t capacity;
 };
 
 // counts[q * (n + 1) + p] for sorted atom p; the trailing slot of each row is 0.
