@@ -198,6 +198,42 @@ __global__ void __launch_bounds__(kPairWarps * 32)
     const int32_t len = grp.end - grp.first < 32 ? grp.end - grp.first : 32;
     const int32_t p = grp.first + (lane < len ? lane : 0);
     const bool mine = lane < len && !b.irr[p];
+    if (EMIT && b.masks) {
+      // Hits recorded by the count pass: expand the stored masks.
+      const int4 hdr = b.task_hdr[task];
+      if (hdr.x == -2) continue;
+      if (hdr.x >= 0) {
+        const int32_t h0 = hdr.y, h1 = hdr.z;
+        const uint32_t pw = (uint32_t)hdr.w;  // three signed 10-bit shifts
+        const int32_t s0 = (int32_t)(pw << 22) >> 22;
+        const int32_t s1 = (int32_t)(pw << 12) >> 22;
+        const int32_t s2 = (int32_t)(pw << 2) >> 22;
+        int64_t slot = mine ? t.base[0] + (offs[(int64_t)p * n_cells + c] - off0) : 0;
+        SlotMeta mi{};
+        if (mine) mi = b.meta[p];
+        for (int32_t jb = h0; jb < h1; jb += 32) {
+          uint32_t hits = mine ? b.masks[(int64_t)hdr.x + (jb - h0) + lane] : 0u;
+          if (!__any_sync(0xffffffffu, hits != 0)) continue;
+          if (jb + lane < h1) smt[lane] = b.meta[jb + lane];
+          __syncwarp();
+          while (hits) {
+            const int jj = __ffs(hits) - 1;
+            hits &= hits - 1;
+            const SlotMeta mj = smt[jj];
+            t.src[0][slot] = (int64_t)mi.orig + t.index_offset;
+            dst0[slot] = (int64_t)mj.orig + t.index_offset;
+            int32_t* sp = t.sh[0] + 3 * slot;
+            sp[0] = (mj.sx - mi.sx) + s0;
+            sp[1] = (mj.sy - mi.sy) + s1;
+            sp[2] = (mj.sz - mi.sz) + s2;
+            ++slot;
+          }
+          __syncwarp();
+        }
+        continue;
+      }
+      // hdr.x == -1: the masks did not fit; recompute below.
+    }
 
     // The stencil cell (shared by the group) and the group's bin centre.
     const char4 st = stencil[c];
@@ -228,7 +264,25 @@ __global__ void __launch_bounds__(kPairWarps * 32)
     uint32_t cnt = 0;
     int64_t slot = 0;
     if (EMIT && mine) slot = t.base[0] + (offs[(int64_t)p * n_cells + c] - off0);
-    if (__any_sync(0xffffffffu, live) && b1 > b0) {
+    const bool work = __any_sync(0xffffffffu, live) && b1 > b0;
+    // Count pass: reserve this task's hit masks (one word per lane per chunk).
+    int32_t mbase = -2;
+    if (!EMIT && b.masks) {
+      if (work) {
+        const int32_t words = ((b1 - b0 + 31) >> 5) * 32;
+        long long top = 0;
+        if (lane == 0) top = (long long)atomicAdd(b.mask_top, (unsigned long long)words);
+        top = __shfl_sync(0xffffffffu, top, 0);
+        const bool fits = top + words <= b.mask_cap && top + words < 0x7fffffffLL &&
+                          sh[0] >= -511 && sh[0] <= 511 && sh[1] >= -511 && sh[1] <= 511 &&
+                          sh[2] >= -511 && sh[2] <= 511;
+        mbase = fits ? (int32_t)top : -1;
+      }
+      if (lane == 0)
+        b.task_hdr[task] = make_int4(mbase, b0, b1,
+                                     (sh[0] & 1023) | ((sh[1] & 1023) << 10) | ((sh[2] & 1023) << 20));
+    }
+    if (work) {
       const float4 a = b.p32[p];
       const int32_t io = __float_as_int(a.w);
       const float ux = __double2float_rn(dsub(cs[0], cb[0])) - a.x;
@@ -276,6 +330,7 @@ __global__ void __launch_bounds__(kPairWarps * 32)
         uint32_t hits = inside & order;
         if (!EMIT) {
           cnt += __popc(hits);
+          if (mbase >= 0) b.masks[(int64_t)mbase + (jb - b0) + lane] = hits;
         } else {
           while (hits) {
             const int jj = __ffs(hits) - 1;

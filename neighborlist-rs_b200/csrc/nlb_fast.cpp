@@ -34,6 +34,7 @@ struct FastKey {
   cudaStream_t stream;
   void* bufs[kSlotCount];
   int64_t capacity;
+  int64_t mask_cap;
   int32_t need_rank;
   int32_t prof;
 };
@@ -44,6 +45,7 @@ struct FastState {
   cudaGraphExec_t exec = nullptr;
   int launches = 0;  // kernels per replay
   int64_t last_m = 0;
+  int64_t last_mask_words = 0;
 };
 
 FastState& state_for(Ctx& c) {
@@ -72,7 +74,7 @@ int64_t estimate_edges(const SystemPlan& sp, double rc) {
 
 // Sizes every workspace buffer of the fast pipeline (may allocate; never
 // inside a capture).
-Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity) {
+Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) {
   const int64_t n = sp.n;
   const int64_t nb = sp.grid.total_bins;
   const int64_t cells = stencil_cells_of(sp.grid);
@@ -84,10 +86,17 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity) {
   b.rank_of_bin = slot<int32_t>(c, kSlotRankTab, nb);
   sp.rank_cached = b.rank_of_bin == tab_before && tab_cap > 0 && c.rank_nb[0] == sp.grid.nb[0] &&
                    c.rank_nb[1] == sp.grid.nb[1] && c.rank_nb[2] == sp.grid.nb[2];
-  int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 2);
+  // Zeroed block: bin histogram, scatter cursors, 2 task counters, 64-bit
+  // mask cursor (8-byte aligned: 2 nb + 2 is even).
+  int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 4);
   b.bin_count = zeroed;
   b.bin_fill = zeroed ? zeroed + nb : nullptr;
   b.counters = zeroed ? zeroed + 2 * nb : nullptr;
+  b.mask_top = zeroed ? reinterpret_cast<unsigned long long*>(zeroed + 2 * nb + 2) : nullptr;
+  const int64_t max_tasks = (n / 32 + std::min<int64_t>(n, nb) + 1) * cells;
+  b.task_hdr = slot<int4>(c, kSlotTaskHdr, max_tasks);
+  b.masks = slot<uint32_t>(c, kSlotMasks, mask_cap);
+  b.mask_cap = mask_cap;
   b.bin_start = slot<int64_t>(c, kSlotBinStart, nb + 1);
   b.key = slot<uint64_t>(c, kSlotKey, n);
   b.rank = slot<int32_t>(c, kSlotRank, n);
@@ -112,7 +121,7 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity) {
   if (!b.rank_of_bin || !zeroed || !b.bin_start || !b.key || !b.rank || !b.skey || !b.sidx ||
       !b.skey2 || !b.sidx2 || !b.px || !b.py || !b.pz || !b.meta || !b.p32 || !b.sbin ||
       !b.groups || !b.irr_list || !b.irr || !b.scan_tmp || !sp.counts || !sp.offs ||
-      !sp.out_src || !sp.out_sh)
+      !sp.out_src || !sp.out_sh || !b.task_hdr || !b.masks)
     return fail(NLB_ERR_NOMEM, "device allocation failed");
   return Status{NLB_OK};
 }
@@ -133,7 +142,7 @@ void issue_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t capacity) {
   const int64_t n = sp.n;
   const int64_t nb = sp.grid.total_bins;
   c.mark(0);
-  cudaMemsetAsync(sp.gb.bin_count, 0, sizeof(int32_t) * (2 * (size_t)nb + 2), s);
+  cudaMemsetAsync(sp.gb.bin_count, 0, sizeof(int32_t) * (2 * (size_t)nb + 4), s);
   launch_grid_build(sp.grid, d_pos, n, sp.gb, s, !sp.rank_cached);
   c.mark(1);
   launch_pair_count(sp.grid, sp.gb, n, sp.band, sp.counts, s);
@@ -156,7 +165,11 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
   const size_t have = c.bufs[kSlotOutSh].cap / (3 * sizeof(int32_t));
   if ((int64_t)have > capacity && c.bufs[kSlotOutEi].cap / (2 * sizeof(int64_t)) >= have)
     capacity = (int64_t)have;
-  Status st = prepare_fast(c, sp, capacity);
+  // Hit-mask arena: the last run's need x 1.25, at least 64 words per atom.
+  int64_t mask_cap = std::max<int64_t>(64 * sp.n + 4096, fs.last_mask_words + fs.last_mask_words / 4);
+  const int64_t mask_have = (int64_t)(c.bufs[kSlotMasks].cap / sizeof(uint32_t));
+  if (mask_have > mask_cap) mask_cap = mask_have;
+  Status st = prepare_fast(c, sp, capacity, mask_cap);
   if (!st.ok()) return st;
 
   FastKey key;
@@ -168,6 +181,7 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
   key.stream = c.stream;
   for (int i = 0; i < kSlotCount; ++i) key.bufs[i] = c.bufs[i].p;
   key.capacity = capacity;
+  key.mask_cap = mask_cap;
   key.need_rank = sp.rank_cached ? 0 : 1;
   key.prof = c.prof ? 1 : 0;
 
@@ -219,6 +233,9 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(c.h_small + 1, sp.gb.scan_tmp + 1, sizeof(int64_t),
                         cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c.h_small + 2, sp.gb.mask_top, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                        c.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
   if (e != cudaSuccess) return cuda_fail(e, "neighbour-list pipeline");
   if (c.h_small[1] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
@@ -240,6 +257,7 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
     fs.have_key = false;  // workspace pointers changed
   }
   fs.last_m = m;
+  fs.last_mask_words = c.h_small[2];
   *m_out = m;
   return Status{NLB_OK};
 }

@@ -50,6 +50,8 @@ enum Slot : int {
   kSlotIrrList,
   kSlotIrr,
   kSlotCounters,
+  kSlotTaskHdr,
+  kSlotMasks,
   kSlotBatch0,  // first slot owned by the batched path
   kSlotCount = kSlotBatch0 + 32,
 };

@@ -50,6 +50,16 @@ struct GridBuffers {
   int32_t* irr_list;
   uint8_t* irr;
   int32_t* counters;
+  // Optional (masks == nullptr: the emit pass recomputes every test): the
+  // count pass stores, per pair task, the candidate range, image shift and a
+  // 32-bit hit mask per lane per 32-candidate chunk in `masks` (bump-
+  // allocated through *mask_top, at most mask_cap words); the emit pass then
+  // only expands bits.  task_hdr[task] = {mask base (-2: nothing to emit,
+  // -1: recompute), b0, b1, packed shift}.
+  int4* task_hdr;
+  uint32_t* masks;
+  unsigned long long* mask_top;
+  int64_t mask_cap;
 };
 
 // need_rank_table = false reuses rank_of_bin from a previous build with the

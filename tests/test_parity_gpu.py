@@ -292,3 +292,34 @@ def test_large_system_many_scan_tiles(nl, oracle):
     small = pos[:20_000] * 0.5
     for rc in (6.0, 3.0, 6.0):
         single(nl, oracle, small, eye(L * 0.5), rc, what=f"grid change rc {rc}")
+
+
+@pytest.mark.parametrize("rc", [6.0, 14.0])
+def test_repeated_calls_graph_replay(nl, oracle, rc):
+    """Identical repeated builds: first direct, then captured, then replayed
+    as a CUDA graph (with the hit-mask and edge arenas resized in between);
+    every result must equal the oracle's."""
+    from neighborlist_rs import workloads as W
+
+    pos, rows = W.cluster_liquid(n_clusters=400, box=33.0, seed=12)
+    ref = oracle.search_single(pos, rows.T, PBC3, rc, nthreads=8)
+    cell = nl.PyCell(rows.T.tolist())
+    for it in range(5):
+        assert_same(nl.build_neighborlists(cell, pos, rc), ref, f"call {it} rc {rc}")
+
+
+def test_torch_device_api(nl, oracle):
+    import torch
+    from neighborlist_rs import workloads as W
+
+    pos, rows = W.cluster_liquid(n_clusters=300, box=30.0, seed=13)
+    cell = nl.PyCell(rows.T.tolist())
+    ref = oracle.search_single(pos, rows.T, PBC3, 6.0, nthreads=8)
+    d = torch.from_numpy(pos).cuda()
+    for it in range(3):
+        r = nl.build_neighborlists_torch(cell, d, 6.0)
+        assert r["edge_index"].is_cuda and r["edge_index"].dtype == torch.int64
+        assert_same({"edge_index": r["edge_index"].cpu().numpy(),
+                     "shift": r["shift"].cpu().numpy()}, ref, f"torch call {it}")
+    r0 = nl.build_neighborlists_torch(cell, d[:0], 6.0)
+    assert r0["edge_index"].shape == (2, 0)
