@@ -422,6 +422,147 @@ def extra_measurements(nl, torch, args):
         "device_ms_phases": {k: v / max(calls, 1) for k, v in ph.items()},
         "plain_per_system_loop_systems_per_s": sample / tp,
         "atoms": int(pb.shape[0]), "edges": mb}
+    out["served"] = served_measurements(nl)
+    return out
+
+
+def run_stream(srv, reqs, rate, seed=0):
+    """Offers `reqs` [(cell, positions, cutoff)] to the server through its
+    Python API (Server.submit / wait, numpy results): Poisson arrivals at
+    `rate` req/s (None: all at once).  One client thread submits each
+    request when it is due and, in between, collects finished results in
+    arrival order (results dropped).  Latency is the server's submit -> done
+    time of each request."""
+    import collections
+
+    n = len(reqs)
+    arrivals = (np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n))
+                if rate else np.zeros(n))
+    lat = np.zeros(n)
+    edges = np.zeros(n, np.int64)
+    pending = collections.deque()
+    t0 = time.perf_counter()
+    i = 0
+    while i < n or pending:
+        now = time.perf_counter() - t0
+        if i < n and arrivals[i] <= now:
+            c, p, rc = reqs[i]
+            pending.append((i, srv.submit(c, p, rc)))
+            i += 1
+            if i == n:
+                t_sub = time.perf_counter() - t0
+            continue
+        if not pending:
+            time.sleep(max(0.0, arrivals[i] - now))
+            continue
+        try:
+            j, t = pending[0]
+            r, ms = srv.wait_timed(t, None if i >= n else max(0.0, arrivals[i] - now))
+        except TimeoutError:
+            continue
+        pending.popleft()
+        lat[j] = ms
+        edges[j] = r["edge_index"].shape[1]
+        del r
+    t = time.perf_counter() - t0
+    return {"offered_req_per_s": rate, "submitted_req_per_s": n / t_sub,
+            "systems_per_s": n / t, "edges_per_s": float(edges.sum()) / t,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "requests": n, "edges": int(edges.sum())}
+
+
+def run_stream_raw(srv, reqs, device=False):
+    """All requests at once through the C ABI with arguments marshalled
+    beforehand (nlb_server_submit / nlb_server_wait / nlb_result_free):
+    the server's capacity without the Python API's per-call cost.  With
+    device=True results stay in HBM and are released right after the wait
+    (no device-to-host copies)."""
+    import ctypes
+
+    import neighborlist_rs as nl
+
+    lib, h = nl._lib, srv._handle()
+    args = []
+    for c, p, rc in reqs:
+        hp, pb = nl._cell_args(c)
+        args.append((p.ctypes.data_as(nl._dp), p.shape[0], hp, pb, float(rc)))
+    r = nl._Result()
+    lat = ctypes.c_double(0.0)
+    lats = np.zeros(len(reqs))
+    m = 0
+    t0 = time.perf_counter()
+    dev = int(device)
+    tickets = [lib.nlb_server_submit(h, a, n, hp, pb, rc, dev) for a, n, hp, pb, rc in args]
+    t_sub = time.perf_counter() - t0
+    for k, t in enumerate(tickets):
+        if lib.nlb_server_wait(h, t, -1.0, ctypes.byref(r), ctypes.byref(lat)) != 0:
+            raise RuntimeError(lib.nlb_last_error().decode())
+        m += r.n_edges
+        lats[k] = lat.value
+        if device:
+            lib.nlb_server_release(h, t)
+        else:
+            lib.nlb_result_free(ctypes.byref(r))
+    t = time.perf_counter() - t0
+    return {"submitted_req_per_s": len(reqs) / t_sub, "systems_per_s": len(reqs) / t,
+            "edges_per_s": m / t, "p50_ms": float(np.percentile(lats, 50)),
+            "p99_ms": float(np.percentile(lats, 99)), "requests": len(reqs), "edges": int(m)}
+
+
+def served_measurements(nl):
+    """Served loop (continuous batching, 40 GB HBM budget): a small-request
+    mix and a bounded sample of the full request-size distribution, each
+    against the plain per-request loop (build_neighborlists) over the same
+    requests.  Every arm runs once untimed over the same requests first."""
+    from neighborlist_rs import workloads as W
+    from neighborlist_rs.serving import Server
+
+    def as_reqs(stream):
+        return [(None if s.cell_rows is None else nl.PyCell(s.cell_rows.T.tolist()),
+                 s.positions, s.cutoff) for s in stream]
+
+    def plain(reqs):
+        t0 = time.perf_counter()
+        m = 0
+        for c, p, rc in reqs:
+            r = nl.build_neighborlists(c, p, rc)
+            m += r["edge_index"].shape[1]
+            del r
+        t = time.perf_counter() - t0
+        return {"systems_per_s": len(reqs) / t, "edges_per_s": m / t, "requests": len(reqs)}
+
+    out = {}
+    small = as_reqs(W.request_stream(4096, seed=21, n_range=(16, 2048)))
+    plain(small[:1024])
+    res = {"plain_per_request_loop": plain(small[:1024])}
+    with Server(hbm_budget_bytes=40 << 30, workers=2, max_batch=4096) as srv:
+        run_stream(srv, small, None)
+        res["saturated_python_api"] = run_stream(srv, small, None)
+        res["saturated_c_abi"] = run_stream_raw(srv, small)
+        run_stream_raw(srv, small, device=True)
+        res["saturated_c_abi_device_results"] = run_stream_raw(srv, small, device=True)
+        for rate in (2000, 10000, 25000):
+            k = min(len(small), max(512, int(rate * 0.4)))
+            res[f"poisson_{rate}"] = run_stream(srv, small[:k], rate, seed=rate)
+        st = srv.stats()
+        res["batches"] = st["batches"]
+        res["largest_batch"] = st["largest_batch"]
+    out["small_mix_4096"] = dict(
+        res, workload="4096 requests, N log-uniform [16, 2048], 70% orthorhombic / 20% "
+                      "triclinic / 10% isolated, rho 0.1, rc in {5, 6, 8}")
+    full = as_reqs(W.request_stream(48, seed=22))
+    plain(full)
+    res = {"plain_per_request_loop": plain(full)}
+    with Server(hbm_budget_bytes=40 << 30, workers=2, max_batch=4096) as srv:
+        run_stream(srv, full, None)
+        res["saturated_python_api"] = run_stream(srv, full, None)
+        res["saturated_c_abi"] = run_stream_raw(srv, full)
+        run_stream_raw(srv, full, device=True)
+        res["saturated_c_abi_device_results"] = run_stream_raw(srv, full, device=True)
+        res["poisson_100"] = run_stream(srv, full, 100, seed=100)
+    out["full_range_sample_48"] = dict(
+        res, workload="48 requests, N log-uniform [16, 1e6] (bounded sample of the "
+                      "served distribution), same cell/density/cutoff mix")
     return out
 
 

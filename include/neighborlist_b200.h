@@ -32,6 +32,7 @@ extern "C" {
 #define NLB_ERR_VALUE 1 /* invalid input; message from nlb_last_error() */
 #define NLB_ERR_CUDA 2  /* CUDA failure (no device, launch or copy error) */
 #define NLB_ERR_NOMEM 3 /* device or pinned-host allocation failed */
+#define NLB_NOT_READY 4 /* nlb_server_wait: the request did not finish in time */
 
 typedef struct nlb_result {
   int64_t n_edges;     /* M */
@@ -83,6 +84,12 @@ void nlb_result_free(nlb_result* r);
 /* Releases one array obtained from a result (for callers that hand the two
  * arrays to separate owners, e.g. two numpy arrays). */
 void nlb_host_free(void* p);
+
+/* Pinned host pool behind every host result (no counterpart in the
+ * reference): fills 7 counters: cudaHostAlloc calls, microseconds spent in
+ * them, bytes they allocated, cudaFreeHost calls, microseconds spent in
+ * them, requests served from cached blocks, bytes cached now. */
+void nlb_pinned_stats(int64_t* out);
 
 /* Dispatch thresholds (src/config.rs:4-40).  The brute-force threshold decides
  * brute force vs cell list and therefore the output order; the parallel
@@ -151,6 +158,49 @@ int64_t nlb_profile_read(double* ms);
 int nlb_build_noalloc(const double* d_positions, int64_t n_atoms, double cutoff,
                       const double* cell, const uint8_t* pbc, int64_t* d_edge_index,
                       int32_t* d_shift, int64_t max_edges, int64_t* n_edges, void* stream);
+
+/* ---- Served request loop (continuous batching). ----
+ * No single counterpart in the reference: it replaces the caller-side loop
+ * that calls search_single (src/single.rs:8-89) once per arriving structure.
+ * Worker threads (n_workers, each with its own stream and workspace on
+ * `device`) take queued requests in arrival order; small requests
+ * (<= 2048 atoms) that fit the HBM budget are run together by the batched
+ * kernels, each with its own cutoff, and larger ones by the single-system
+ * pipeline.  Every result equals nlb_build of the same request.
+ *
+ * nlb_server_create: hbm_budget_bytes bounds the estimated device footprint
+ *   of admitted requests (positions, workspace, edges; device-resident
+ *   results stay counted until released); max_batch bounds the systems per
+ *   batch.  NULL on error (nlb_last_error).
+ * nlb_server_submit: copies the positions; cell/pbc as in nlb_build.
+ *   device_result != 0 keeps the result in HBM (nlb_result then holds device
+ *   pointers).  Returns a ticket > 0, or -code on a rejected request (invalid
+ *   input, or an estimate larger than the whole budget).
+ * nlb_server_wait: timeout_s < 0 waits for good.  Returns NLB_OK and fills
+ *   *out (and *latency_ms, submit -> done) when the request finished,
+ *   NLB_NOT_READY on timeout, or the request's error code (nlb_last_error
+ *   has its message).  Host results then belong to the caller (nlb_result_free) and
+ *   the ticket is retired; device results stay owned by the server until
+ *   nlb_server_release, which the caller issues once its own work reading
+ *   them has completed.
+ * nlb_server_stats: fills 13 counters: submitted, completed, failed, batches,
+ *   HBM bytes reserved, queued requests, largest batch, budget, then worker
+ *   wall time in microseconds (all workers) spent in: batch staging and
+ *   launches, waiting for the count pass, issuing result copies, waiting
+ *   for the emit pass and copies, large requests.
+ * nlb_server_destroy: cancels queued requests, lets running ones finish,
+ *   joins the workers (freeing their workspaces) and frees every result that
+ *   was not handed over.  No thread may be inside nlb_server_wait then. */
+typedef struct nlb_server nlb_server;
+nlb_server* nlb_server_create(int device, int64_t hbm_budget_bytes, int n_workers, int max_batch);
+int64_t nlb_server_submit(nlb_server* server, const double* positions, int64_t n_atoms,
+                          const double* cell, const uint8_t* pbc, double cutoff,
+                          int device_result);
+int nlb_server_wait(nlb_server* server, int64_t ticket, double timeout_s, nlb_result* out,
+                    double* latency_ms);
+int nlb_server_release(nlb_server* server, int64_t ticket);
+void nlb_server_stats(nlb_server* server, int64_t* stats);
+void nlb_server_destroy(nlb_server* server);
 
 /* Cell helpers behind the Python PyCell class (src/python_api.rs:15-99).
  * nlb_cell_check: 0 if H is invertible, NLB_ERR_VALUE ("Cell matrix is not

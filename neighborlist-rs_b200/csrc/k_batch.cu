@@ -19,14 +19,18 @@
 // Per-atom counts of all systems form one flat row per cutoff; one exclusive
 // scan gives every system's global edge offsets, so the emit pass writes the
 // concatenated, exact-sized output (systems in input order) directly.
+#include <algorithm>
+#include <vector>
+
 #include "k_traverse.cuh"
 
 namespace nlb {
 
 namespace {
 
-constexpr int kBatchThreads = 256;
-constexpr int kBatchWarps = kBatchThreads / 32;
+constexpr int kBatchThreads = 256;       // CTA size for systems of <= kBatchLargeAtoms
+constexpr int kBatchLargeThreads = 512;  // CTA size for larger systems
+constexpr int kBatchChunk = 256;         // atoms per work item of a larger system
 
 __device__ __forceinline__ double dfmin(double a, double b) {
   if (a != a) return b;
@@ -111,11 +115,13 @@ __device__ void dev_plan_grid(const double* w, double rc, GridParams& g) {
 __global__ void k_plan(const double* __restrict__ pos, const int64_t* __restrict__ starts,
                        int32_t s0, int32_t s1, const double* __restrict__ cells,
                        const uint8_t* __restrict__ pbcs, const uint8_t* __restrict__ has_cell,
-                       double rc_max, uint64_t bf_threshold, int multi, int64_t run_start,
-                       SysPlan* __restrict__ plans, int32_t* __restrict__ error_flag) {
+                       double rc_max_all, uint64_t bf_threshold, int multi, int64_t run_start,
+                       SysPlan* __restrict__ plans, int32_t* __restrict__ error_flag,
+                       const double* __restrict__ sys_rc) {
   const int lane = threadIdx.x & 31;
   const int32_t s = s0 + blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   if (s >= s1) return;
+  const double rc_max = sys_rc ? sys_rc[s] : rc_max_all;
   const int64_t b = starts[s], e = starts[s + 1];
   const bool own_cell = cells && has_cell && has_cell[s];
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -139,6 +145,7 @@ __global__ void k_plan(const double* __restrict__ pos, const int64_t* __restrict
   P.start = b;
   P.n = (int32_t)(e - b);
   P.slot = b - run_start;
+  P.rc_sq = dmul(rc_max, rc_max);
   GridParams& g = P.g;
   for (int i = 0; i < 9; ++i) g.h[i] = 0.0;
   if (own_cell) {
@@ -413,14 +420,15 @@ __device__ __forceinline__ void visit_smem_brute_atom(const SysPlan& P, const Sm
   }
 }
 
-// Pulls the next system index (in work order) for the whole CTA; -1 when done.
-__device__ __forceinline__ int next_system(int* work, const int32_t* order, int n_sys) {
+// Pulls the next work item (system, first atom) for the whole CTA; system -1
+// when the queue is empty.
+__device__ __forceinline__ int2 next_item(int* work, const int2* items, int n_items) {
   __shared__ int s_next;
   if (threadIdx.x == 0) s_next = atomicAdd(work, 1);
   __syncthreads();
   const int w = s_next;
   __syncthreads();
-  return w < n_sys ? order[w] : -1;
+  return w < n_items ? items[w] : make_int2(-1, 0);
 }
 
 __device__ __forceinline__ void load_plan(const SysPlan* plans, int s, SysPlan& sp_smem) {
@@ -431,68 +439,130 @@ __device__ __forceinline__ void load_plan(const SysPlan* plans, int s, SysPlan& 
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBatchThreads)
-    k_batch_count(const SysPlan* __restrict__ plans, const int32_t* __restrict__ order, int n_sys,
-                  const double* __restrict__ pos, int cap, CutoffSet cs,
+// Per-system cutoff (CutoffSet.k == 0): the pass's single cutoff is the
+// system's own (SysPlan.rc_sq).
+__device__ __forceinline__ void system_cutoff(const CutoffSet& cs, const SysPlan& P,
+                                              CutoffSet& out) {
+  out = cs;
+  out.k = 1;
+  out.rc_sq[0] = P.rc_sq;
+  out.max_sq = P.rc_sq;
+  out.lower_sq = -1.0;
+  out.disjoint = 0;
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS)
+    k_batch_count(const SysPlan* __restrict__ plans, const int2* __restrict__ items, int n_items,
+                  int chunk, const double* __restrict__ pos, int cap, CutoffSet cs,
                   uint32_t* __restrict__ counts, int64_t row, int* __restrict__ work) {
+  constexpr int kWarps = THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ SysPlan P;
+  __shared__ CutoffSet cs_sys;
   const SmemView v = smem_view(smem, cap);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (;;) {
-    const int s = next_system(work, order, n_sys);
-    if (s < 0) break;
-    load_plan(plans, s, P);
+    const int2 item = next_item(work, items, n_items);
+    if (item.x < 0) break;
+    load_plan(plans, item.x, P);
     if (P.method < 0) continue;
+    const CutoffSet* csp = &cs;
+    if (cs.k == 0) {
+      if (threadIdx.x == 0) system_cutoff(cs, P, cs_sys);
+      __syncthreads();
+      csp = &cs_sys;
+    }
     load_system(P, pos, v);
-    for (int p = warp; p < P.n; p += kBatchWarps) {
-      CountSink sink{&cs, 0u};
+    const int p_end = min(P.n, item.y + chunk);
+    for (int p = item.y + warp; p < p_end; p += kWarps) {
+      CountSink sink{csp, 0u};
       if (P.method == 2)
-        visit_smem_grid_atom(P, v, p, cs.max_sq, sink);
+        visit_smem_grid_atom(P, v, p, csp->max_sq, sink);
       else
-        visit_smem_brute_atom(P, v, p, cs.max_sq, sink);
-      if (lane < cs.k) counts[(int64_t)lane * row + P.slot + p] = sink.cnt;
+        visit_smem_brute_atom(P, v, p, csp->max_sq, sink);
+      if (lane < csp->k) counts[(int64_t)lane * row + P.slot + p] = sink.cnt;
     }
     __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(kBatchThreads)
-    k_batch_emit(const SysPlan* __restrict__ plans, const int32_t* __restrict__ order, int n_sys,
-                 const double* __restrict__ pos, int cap, CutoffSet cs,
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS)
+    k_batch_emit(const SysPlan* __restrict__ plans, const int2* __restrict__ items, int n_items,
+                 int chunk, const double* __restrict__ pos, int cap, CutoffSet cs,
                  const int64_t* __restrict__ offs, int64_t row, EmitTargets t,
                  int* __restrict__ work) {
+  constexpr int kWarps = THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ SysPlan P;
+  __shared__ CutoffSet cs_sys;
+  __shared__ EmitTargets1 t_blk;
   const SmemView v = smem_view(smem, cap);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool blocks = t.system_blocks && cs.k == 0;
   for (;;) {
-    const int s = next_system(work, order, n_sys);
-    if (s < 0) break;
-    load_plan(plans, s, P);
+    const int2 item = next_item(work, items, n_items);
+    if (item.x < 0) break;
+    load_plan(plans, item.x, P);
     if (P.method < 0) continue;
+    const CutoffSet* csp = &cs;
+    if (cs.k == 0) {
+      if (threadIdx.x == 0) {
+        system_cutoff(cs, P, cs_sys);
+        if (blocks) {
+          // This system's edges e in [b0, b0 + m): sources at 2 b0 + (e - b0),
+          // destinations at 2 b0 + m + (e - b0).
+          const int64_t b0 = offs[P.slot] - offs[0];
+          const int64_t m = offs[P.slot + P.n] - offs[P.slot];
+          t_blk.src[0] = t.src[0] + b0;
+          t_blk.dst[0] = t.src[0] + b0 + m;
+          t_blk.sh[0] = t.sh[0];
+        }
+      }
+      __syncthreads();
+      csp = &cs_sys;
+    }
     load_system(P, pos, v);
-    for (int p = warp; p < P.n; p += kBatchWarps) {
+    const int64_t idx_off = t.local_indices ? t.index_offset : P.start + t.index_offset;
+    const int p_end = min(P.n, item.y + chunk);
+    for (int p = item.y + warp; p < p_end; p += kWarps) {
       int64_t cur = 0;
-      if (lane < cs.k) {
+      if (lane < csp->k) {
         const int64_t r = (int64_t)lane * row;
         cur = t.base[lane] + (offs[r + P.slot + p] - offs[r]);
       }
-      EmitSink sink{&cs, &t, cur, P.start};
-      if (P.method == 2)
-        visit_smem_grid_atom(P, v, p, cs.max_sq, sink);
-      else
-        visit_smem_brute_atom(P, v, p, cs.max_sq, sink);
+      if (blocks) {
+        EmitSinkT<EmitTargets1> sink{csp, &t_blk, cur, idx_off};
+        if (P.method == 2)
+          visit_smem_grid_atom(P, v, p, csp->max_sq, sink);
+        else
+          visit_smem_brute_atom(P, v, p, csp->max_sq, sink);
+      } else {
+        EmitSink sink{csp, &t, cur, idx_off};
+        if (P.method == 2)
+          visit_smem_grid_atom(P, v, p, csp->max_sq, sink);
+        else
+          visit_smem_brute_atom(P, v, p, csp->max_sq, sink);
+      }
     }
     __syncthreads();
   }
 }
 
-int grid_for(const void* func, size_t smem) {
+__global__ void k_sys_bounds(const SysPlan* __restrict__ plans, int n_sys,
+                             const int64_t* __restrict__ offs, int64_t row,
+                             int64_t* __restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n_sys) out[s] = offs[plans[s].slot] - offs[0];
+  if (s == n_sys) out[s] = offs[row - 1] - offs[0];
+}
+
+int grid_for(const void* func, int threads, size_t smem) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kBatchThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem);
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
@@ -507,34 +577,95 @@ size_t batch_smem_bytes(int cap) {
 void launch_plan(const double* pos, const int64_t* starts, int32_t s0, int32_t s1,
                  const double* cells, const uint8_t* pbcs, const uint8_t* has_cell, double rc_max,
                  uint64_t bf_threshold, int multi, int64_t run_start, SysPlan* plans,
-                 int32_t* error_flag, cudaStream_t s) {
+                 int32_t* error_flag, cudaStream_t s, const double* sys_rc) {
   const int per_block = 8;
   const unsigned blocks = (unsigned)((s1 - s0 + per_block - 1) / per_block);
   k_plan<<<blocks, per_block * 32, 0, s>>>(pos, starts, s0, s1, cells, pbcs, has_cell, rc_max,
-                                           bf_threshold, multi, run_start, plans, error_flag);
+                                           bf_threshold, multi, run_start, plans, error_flag,
+                                           sys_rc);
   note_launches(1);
 }
 
-void launch_batch_count(const SysPlan* plans, const int32_t* order, int n_sys, const double* pos,
-                        int cap, const CutoffSet& cs, uint32_t* counts, int64_t row, int* work,
+void launch_sys_bounds(const SysPlan* plans, int n_sys, const int64_t* offs, int64_t row,
+                       int64_t* out, cudaStream_t s) {
+  k_sys_bounds<<<(unsigned)((n_sys + 1 + 127) / 128), 128, 0, s>>>(plans, n_sys, offs, row, out);
+  note_launches(1);
+}
+
+void launch_batch_count(const SysPlan* plans, const BatchItems& w, const double* pos,
+                        const CutoffSet& cs, uint32_t* counts, int64_t row, int* work2,
                         cudaStream_t s) {
-  const size_t smem = batch_smem_bytes(cap);
-  ensure_smem_attr((const void*)k_batch_count, (int)smem);
-  const int grid = std::min(grid_for((const void*)k_batch_count, smem), std::max(n_sys, 1));
-  k_batch_count<<<grid, kBatchThreads, smem, s>>>(plans, order, n_sys, pos, cap, cs, counts, row,
-                                                  work);
-  note_launches(1);
+  if (w.n_large > 0) {
+    const size_t smem = batch_smem_bytes(w.cap_large);
+    auto k = k_batch_count<kBatchLargeThreads>;
+    ensure_smem_attr((const void*)k, (int)smem);
+    const int grid = std::min(grid_for((const void*)k, kBatchLargeThreads, smem), w.n_large);
+    k<<<grid, kBatchLargeThreads, smem, s>>>(plans, w.items, w.n_large, kBatchChunk, pos,
+                                             w.cap_large, cs, counts, row, work2);
+    note_launches(1);
+  }
+  if (w.n_small > 0) {
+    const size_t smem = batch_smem_bytes(w.cap_small);
+    auto k = k_batch_count<kBatchThreads>;
+    ensure_smem_attr((const void*)k, (int)smem);
+    const int grid = std::min(grid_for((const void*)k, kBatchThreads, smem), w.n_small);
+    k<<<grid, kBatchThreads, smem, s>>>(plans, w.items + w.n_large, w.n_small, 1 << 30, pos,
+                                        w.cap_small, cs, counts, row, work2 + 1);
+    note_launches(1);
+  }
 }
 
-void launch_batch_emit(const SysPlan* plans, const int32_t* order, int n_sys, const double* pos,
-                       int cap, const CutoffSet& cs, const int64_t* offs, int64_t row,
-                       const EmitTargets& t, int* work, cudaStream_t s) {
-  const size_t smem = batch_smem_bytes(cap);
-  ensure_smem_attr((const void*)k_batch_emit, (int)smem);
-  const int grid = std::min(grid_for((const void*)k_batch_emit, smem), std::max(n_sys, 1));
-  k_batch_emit<<<grid, kBatchThreads, smem, s>>>(plans, order, n_sys, pos, cap, cs, offs, row, t,
-                                                 work);
-  note_launches(1);
+void launch_batch_emit(const SysPlan* plans, const BatchItems& w, const double* pos,
+                       const CutoffSet& cs, const int64_t* offs, int64_t row,
+                       const EmitTargets& t, int* work2, cudaStream_t s) {
+  if (w.n_large > 0) {
+    const size_t smem = batch_smem_bytes(w.cap_large);
+    auto k = k_batch_emit<kBatchLargeThreads>;
+    ensure_smem_attr((const void*)k, (int)smem);
+    const int grid = std::min(grid_for((const void*)k, kBatchLargeThreads, smem), w.n_large);
+    k<<<grid, kBatchLargeThreads, smem, s>>>(plans, w.items, w.n_large, kBatchChunk, pos,
+                                             w.cap_large, cs, offs, row, t, work2);
+    note_launches(1);
+  }
+  if (w.n_small > 0) {
+    const size_t smem = batch_smem_bytes(w.cap_small);
+    auto k = k_batch_emit<kBatchThreads>;
+    ensure_smem_attr((const void*)k, (int)smem);
+    const int grid = std::min(grid_for((const void*)k, kBatchThreads, smem), w.n_small);
+    k<<<grid, kBatchThreads, smem, s>>>(plans, w.items + w.n_large, w.n_small, 1 << 30, pos,
+                                        w.cap_small, cs, offs, row, t, work2 + 1);
+    note_launches(1);
+  }
+}
+
+void plan_batch_items(const int64_t* sizes, int n_sys, std::vector<int2>& items, BatchItems& w) {
+  std::vector<int32_t> order(n_sys);
+  for (int i = 0; i < n_sys; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t x, int32_t y) { return sizes[x] > sizes[y]; });
+  items.clear();
+  w = BatchItems{};
+  int64_t max_large = 0, max_small = 0;
+  for (int32_t i : order) {
+    const int64_t n = sizes[i];
+    if (n > kBatchLargeAtoms) {
+      for (int64_t a = 0; a < n; a += kBatchChunk) items.push_back(make_int2(i, (int)a));
+      max_large = std::max(max_large, n);
+    }
+  }
+  w.n_large = (int)items.size();
+  for (int32_t i : order) {
+    const int64_t n = sizes[i];
+    if (n <= kBatchLargeAtoms) {
+      items.push_back(make_int2(i, 0));
+      max_small = std::max(max_small, n);
+    }
+  }
+  w.n_small = (int)items.size() - w.n_large;
+  w.cap_large = 32;
+  while (w.cap_large < max_large) w.cap_large <<= 1;
+  w.cap_small = 32;
+  while (w.cap_small < max_small) w.cap_small <<= 1;
 }
 
 }  // namespace nlb

@@ -40,10 +40,18 @@ struct CountSink {
   }
 };
 
+// Destinations of one list (served requests: one system's [src | dst] block).
+struct EmitTargets1 {
+  int64_t* src[1];
+  int64_t* dst[1];
+  int32_t* sh[1];
+};
+
 // Hit sink for the emit pass: lane q holds cutoff q's next write slot.
-struct EmitSink {
+template <class Targets>
+struct EmitSinkT {
   const CutoffSet* cs;
-  const EmitTargets* t;
+  const Targets* t;
   int64_t cursor;  // lane q: next slot of cutoff q
   int64_t idx_off = 0;  // added to both atom indices
   __device__ __forceinline__ void operator()(bool hit, double d2, int32_t io, int32_t jo,
@@ -72,5 +80,6 @@ struct EmitSink {
     }
   }
 };
+using EmitSink = EmitSinkT<EmitTargets>;
 
 }  // namespace nlb

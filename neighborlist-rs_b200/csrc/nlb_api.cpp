@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -67,13 +68,103 @@ namespace {
 
 struct PinnedPool {
   std::mutex mu;
+  // Blocks up to 2^kMaxShift bytes: power-of-two classes carved from
+  // kChunk-byte pinned chunks; a released block goes to its class's free
+  // list and is never returned to the system.  cudaHostAlloc is slow (tens
+  // of ms) and serialises with other CUDA calls, so steady-state traffic
+  // must not reach it.
+  static constexpr int kMinShift = 12;  // 4 KB: every block 4 KB aligned
+  static constexpr int kMaxShift = 28;  // 256 MB
+  static constexpr size_t kChunk = size_t(512) << 20;
+  std::vector<void*> free_class[kMaxShift + 1];
+  std::unordered_map<void*, int> class_of;  // class blocks handed out
+  char* bump = nullptr;
+  size_t bump_left = 0;
+  // Larger blocks: dedicated allocations, cached by size (up to kMaxCached).
   std::multimap<size_t, void*> free_blocks;  // size -> block
-  std::unordered_map<void*, size_t> sizes;   // every block handed out or cached
+  std::unordered_map<void*, size_t> sizes;   // every dedicated block
   size_t cached = 0;
   static constexpr size_t kMaxCached = size_t(8) << 30;
+  // Counters (nlb_pinned_stats).
+  int64_t n_host_alloc = 0, us_host_alloc = 0, bytes_host_alloc = 0;
+  int64_t n_host_free = 0, us_host_free = 0, n_hits = 0;
+
+  static int class_for(size_t bytes) {
+    int k = kMinShift;
+    while ((size_t(1) << k) < bytes) ++k;
+    return k;
+  }
+
+  void* host_alloc(size_t bytes) {
+    void* p = nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    const int64_t us = std::chrono::duration_cast<std::chrono::microseconds>(
+                           std::chrono::steady_clock::now() - t0).count();
+    std::lock_guard<std::mutex> lk(mu);
+    ++n_host_alloc;
+    us_host_alloc += us;
+    bytes_host_alloc += (int64_t)bytes;
+    return p;
+  }
+
+  // Splits the rest of the current chunk into free class blocks, largest
+  // first (every block size is a multiple of 4 KB, so all stay 4 KB aligned).
+  void retire_chunk_locked() {
+    for (int k = kMaxShift; k >= kMinShift && bump_left; --k) {
+      const size_t b = size_t(1) << k;
+      while (bump_left >= b) {
+        free_class[k].push_back(bump);
+        bump += b;
+        bump_left -= b;
+      }
+    }
+    bump = nullptr;
+    bump_left = 0;
+  }
+
+  // Takes a class-k block from the free list or the current chunk (under mu).
+  void* take_class_locked(int k) {
+    if (!free_class[k].empty()) {
+      void* p = free_class[k].back();
+      free_class[k].pop_back();
+      ++n_hits;
+      return p;
+    }
+    const size_t b = size_t(1) << k;
+    if (bump_left >= b) {
+      void* p = bump;
+      bump += b;
+      bump_left -= b;
+      return p;
+    }
+    return nullptr;
+  }
 
   void* alloc(size_t bytes) {
     bytes = std::max<size_t>(bytes, 256);
+    if (bytes <= (size_t(1) << kMaxShift)) {
+      const int k = class_for(bytes);
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        if (void* p = take_class_locked(k)) {
+          class_of[p] = k;
+          return p;
+        }
+      }
+      void* chunk = host_alloc(kChunk);
+      if (!chunk) return nullptr;
+      std::lock_guard<std::mutex> lk(mu);
+      retire_chunk_locked();
+      bump = static_cast<char*>(chunk);
+      bump_left = kChunk;
+      void* p = take_class_locked(k);
+      class_of[p] = k;
+      return p;
+    }
     {
       std::lock_guard<std::mutex> lk(mu);
       auto it = free_blocks.lower_bound(bytes);
@@ -81,22 +172,65 @@ struct PinnedPool {
         void* p = it->second;
         cached -= it->first;
         free_blocks.erase(it);
+        ++n_hits;
         return p;
       }
     }
-    void* p = nullptr;
-    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
+    void* p = host_alloc(bytes);
+    if (!p) return nullptr;
     std::lock_guard<std::mutex> lk(mu);
     sizes[p] = bytes;
     return p;
   }
 
+  // Pre-carves chunks so that the first `bytes` of class traffic do not
+  // wait for cudaHostAlloc.
+  void reserve(size_t bytes) {
+    size_t have = 0;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      have = bump_left;
+      for (int k = kMinShift; k <= kMaxShift; ++k) have += free_class[k].size() << k;
+    }
+    while (have < bytes) {
+      void* chunk = host_alloc(kChunk);
+      if (!chunk) return;
+      std::lock_guard<std::mutex> lk(mu);
+      retire_chunk_locked();
+      bump = static_cast<char*>(chunk);
+      bump_left = kChunk;
+      have += kChunk;
+    }
+  }
+
+  // Slices: results that point into a shared block (one device-to-host copy
+  // for many results); the block returns to the pool with its last slice.
+  std::unordered_map<void*, void*> slice_block;
+  std::unordered_map<void*, int64_t> block_refs;
+
+  void share(void* block, void* slice) {
+    std::lock_guard<std::mutex> lk(mu);
+    slice_block[slice] = block;
+    ++block_refs[block];
+  }
+
   void release(void* p) {
     if (!p) return;
     std::lock_guard<std::mutex> lk(mu);
+    auto sl = slice_block.find(p);
+    if (sl != slice_block.end()) {
+      void* block = sl->second;
+      slice_block.erase(sl);
+      if (--block_refs[block] > 0) return;
+      block_refs.erase(block);
+      p = block;
+    }
+    auto ck = class_of.find(p);
+    if (ck != class_of.end()) {
+      free_class[ck->second].push_back(p);
+      class_of.erase(ck);
+      return;
+    }
     auto it = sizes.find(p);
     if (it == sizes.end()) return;  // not ours
     const size_t sz = it->second;
@@ -104,7 +238,11 @@ struct PinnedPool {
       auto big = std::prev(free_blocks.end());
       cached -= big->first;
       sizes.erase(big->second);
+      const auto t0 = std::chrono::steady_clock::now();
       cudaFreeHost(big->second);
+      us_host_free += std::chrono::duration_cast<std::chrono::microseconds>(
+                          std::chrono::steady_clock::now() - t0).count();
+      ++n_host_free;
       free_blocks.erase(big);
     }
     free_blocks.emplace(sz, p);
@@ -121,6 +259,24 @@ PinnedPool& pinned_pool() {
 
 void* pinned_alloc(size_t bytes) { return pinned_pool().alloc(bytes); }
 void pinned_release(void* p) { pinned_pool().release(p); }
+void pinned_share(void* block, void* slice) { pinned_pool().share(block, slice); }
+
+void pinned_reserve(size_t bytes) { pinned_pool().reserve(bytes); }
+
+void pinned_stats(int64_t* out) {
+  PinnedPool& p = pinned_pool();
+  std::lock_guard<std::mutex> lk(p.mu);
+  out[0] = p.n_host_alloc;
+  out[1] = p.us_host_alloc;
+  out[2] = p.bytes_host_alloc;
+  out[3] = p.n_host_free;
+  out[4] = p.us_host_free;
+  out[5] = p.n_hits;
+  size_t cached = p.cached + p.bump_left;
+  for (int k = PinnedPool::kMinShift; k <= PinnedPool::kMaxShift; ++k)
+    cached += p.free_class[k].size() << k;
+  out[6] = (int64_t)cached;
+}
 
 // ------------------------------------------------------------------ context
 
@@ -141,8 +297,32 @@ void* Ctx::raw(int slot, size_t bytes) {
   return b.p;
 }
 
+namespace {
+thread_local std::unordered_map<int, Ctx*> tl_ctxs;
+}  // namespace
+
+void release_thread_ctx() {
+  release_fast_states();
+  for (auto& kv : tl_ctxs) {
+    Ctx* c = kv.second;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->own_stream);
+    for (Ctx::Buf& b : c->bufs)
+      if (b.p) cudaFree(b.p);
+    for (cudaEvent_t ev : c->ev)
+      if (ev) cudaEventDestroy(ev);
+    if (c->h_small) cudaFreeHost(c->h_small);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    cudaSetDevice(prev);
+    delete c;
+  }
+  tl_ctxs.clear();
+}
+
 Status get_ctx(Ctx** out) {
-  thread_local std::unordered_map<int, Ctx*> ctxs;
+  auto& ctxs = tl_ctxs;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice (is a CUDA device present?)");
@@ -151,7 +331,7 @@ Status get_ctx(Ctx** out) {
   if (it != ctxs.end()) {
     c = it->second;
   } else {
-    c = new Ctx();  // lives for the thread's lifetime; never freed at exit
+    c = new Ctx();  // lives until release_thread_ctx (server workers) or process exit
     c->device = dev;
     e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
@@ -642,6 +822,10 @@ void nlb_result_free(nlb_result* r) {
 }
 
 void nlb_host_free(void* p) { pinned_release(p); }
+
+void nlb_pinned_stats(int64_t* out) {
+  if (out) pinned_stats(out);
+}
 
 int nlb_build_device(const double* d_positions, int64_t n_atoms, double cutoff,
                      const double* cell, const uint8_t* pbc, nlb_device_result* out) {

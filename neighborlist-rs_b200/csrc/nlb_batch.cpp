@@ -89,28 +89,26 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
   const int64_t run_atoms = starts[b] - run_start;
   const int64_t row = run_atoms + 1;
 
+  // Work items, largest systems first for load balance across the
+  // persistent CTAs (larger systems split into chunks of atoms).
+  std::vector<int64_t> sizes(ns);
+  for (int32_t i = 0; i < ns; ++i) sizes[i] = starts[a + i + 1] - starts[a + i];
+  std::vector<int2> items;
+  BatchItems bw;
+  plan_batch_items(sizes.data(), ns, items, bw);
+
   SysPlan* plans = slot<SysPlan>(c, kSlotBatch0 + 0, ns);
-  int32_t* order_d = slot<int32_t>(c, kSlotBatch0 + 1, ns);
-  int32_t* flags = slot<int32_t>(c, kSlotBatch0 + 2, 2);  // [0] plan error, [1] work counter
+  int2* items_d = slot<int2>(c, kSlotBatch0 + 1, items.size());
+  int32_t* flags = slot<int32_t>(c, kSlotBatch0 + 2, 3);  // [0] plan error, [1..2] work counters
   uint32_t* counts = slot<uint32_t>(c, kSlotBatch0 + 3, (size_t)k * row);
   int64_t* offs = slot<int64_t>(c, kSlotBatch0 + 4, (size_t)k * row + 1);
   int64_t* scan_tmp = slot<int64_t>(c, kSlotBatch0 + 5, scan_tmp_elems((int64_t)k * row));
-  if (!plans || !order_d || !flags || !counts || !offs || !scan_tmp)
+  if (!plans || !items_d || !flags || !counts || !offs || !scan_tmp)
     return fail(NLB_ERR_NOMEM, "device allocation failed");
+  bw.items = items_d;
 
-  // Largest systems first for load balance across the persistent CTAs.
-  std::vector<int32_t> order(ns);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
-    return starts[a + x + 1] - starts[a + x] > starts[a + y + 1] - starts[a + y];
-  });
-  int64_t max_n = 1;
-  for (int32_t i = a; i < b; ++i) max_n = std::max<int64_t>(max_n, starts[i + 1] - starts[i]);
-  int cap = 32;
-  while (cap < max_n) cap <<= 1;
-
-  cudaMemcpyAsync(order_d, order.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, s);
-  cudaMemsetAsync(flags, 0, sizeof(int32_t) * 2, s);
+  cudaMemcpyAsync(items_d, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s);
+  cudaMemsetAsync(flags, 0, sizeof(int32_t) * 3, s);
   cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)k * row, s);
   c.mark(0);
   launch_plan(d_pos, d_starts, a, b, d_cells, d_pbcs, d_has, rc_max, g_bf_threshold.load(),
@@ -118,9 +116,8 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
   c.mark(1);
   for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
     const CutoffSet cs = make_pass(rc_sq, g0, disjoint);
-    cudaMemsetAsync(flags + 1, 0, sizeof(int32_t), s);
-    launch_batch_count(plans, order_d, ns, d_pos, cap, cs, counts + (size_t)g0 * row, row,
-                       flags + 1, s);
+    cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
+    launch_batch_count(plans, bw, d_pos, cs, counts + (size_t)g0 * row, row, flags + 1, s);
   }
   c.mark(2);
   exclusive_scan_u32(counts, (int64_t)k * row, offs, scan_tmp, s);
@@ -159,9 +156,8 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
       t.sh[q] = static_cast<int32_t*>(out.shf[g0 + q].p);
       t.base[q] = out.total[g0 + q];
     }
-    cudaMemsetAsync(flags + 1, 0, sizeof(int32_t), s);
-    launch_batch_emit(plans, order_d, ns, d_pos, cap, cs, offs + (size_t)g0 * row, row, t,
-                      flags + 1, s);
+    cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
+    launch_batch_emit(plans, bw, d_pos, cs, offs + (size_t)g0 * row, row, t, flags + 1, s);
   }
   c.mark(5);
   if (c.prof) c.prof_pending_emit = true;

@@ -48,10 +48,9 @@ struct FastState {
   int64_t last_mask_words = 0;
 };
 
-FastState& state_for(Ctx& c) {
-  static thread_local FastState states[16];
-  return states[c.device & 15];
-}
+thread_local FastState tl_states[16];
+
+FastState& state_for(Ctx& c) { return tl_states[c.device & 15]; }
 
 int64_t stencil_cells_of(const GridParams& g) {
   return (int64_t)(2 * g.ns[0] + 1) * (2 * g.ns[1] + 1) * (2 * g.ns[2] + 1);
@@ -71,6 +70,13 @@ int64_t estimate_edges(const SystemPlan& sp, double rc) {
 }
 
 }  // namespace
+
+void release_fast_states() {
+  for (FastState& fs : tl_states) {
+    if (fs.exec) cudaGraphExecDestroy(fs.exec);
+    fs = FastState();
+  }
+}
 
 // Sizes every workspace buffer of the fast pipeline (may allocate; never
 // inside a capture).

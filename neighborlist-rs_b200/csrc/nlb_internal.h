@@ -88,6 +88,10 @@ struct Ctx {
 };
 
 Status get_ctx(Ctx** out);
+// Frees the calling thread's contexts and fast-path graphs (threads that end
+// before the process does, e.g. server workers).
+void release_thread_ctx();
+void release_fast_states();
 bool fp32_search_enabled();
 
 template <class T>
@@ -97,6 +101,13 @@ inline T* slot(Ctx& c, int s, size_t count) {
 
 void* pinned_alloc(size_t bytes);
 void pinned_release(void* p);
+// Registers `slice` (a pointer into pool block `block`, distinct from every
+// other live slice) as a handle of its own: pinned_release(slice) drops it,
+// and the block returns to the pool when its last slice is released.  The
+// block itself must then not be released directly.
+void pinned_share(void* block, void* slice);
+void pinned_stats(int64_t* out);
+void pinned_reserve(size_t bytes);
 
 // One system after planning: cell, dispatch decision, grid or brute-force
 // parameters, cutoffs in ascending order, and (after count_system) the

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "nlb_common.cuh"
@@ -87,6 +88,13 @@ struct EmitTargets {
   // nothing is written if M > capacity (the caller grows and re-emits).
   const int64_t* total_dev;
   int64_t capacity;
+  // Batched kernels: 1 = atom indices local to each system (served requests),
+  // 0 = global indices (system start added).
+  int32_t local_indices;
+  // Batched kernels with per-system cutoffs: 1 = each system's list is one
+  // contiguous [src | dst] block starting at src[0] + 2 * (its first edge
+  // slot), with shifts at sh[0] + 3 * slot as usual (served requests).
+  int32_t system_blocks;
 };
 
 // counts[q * (n + 1) + p] for sorted atom p; the trailing slot of each row is 0.
@@ -140,23 +148,40 @@ struct SysPlan {
   int64_t start;     // first atom of the system (global index)
   int32_t n;         // atoms
   int32_t slot;      // first count slot of the system inside its run
+  double rc_sq;      // the system's own squared cutoff (per-system cutoff runs)
 };
 
 size_t batch_smem_bytes(int cap);
 // Plans systems [s0, s1): plans[s - s0].  error_flag: 1 = singular cell,
 // 2 = stencil too large.
+// sys_rc (optional, indexed like starts): a cutoff per system; the count /
+// emit launches then take a CutoffSet with k == 0 and use each plan's rc_sq.
 void launch_plan(const double* pos, const int64_t* starts, int32_t s0, int32_t s1,
                  const double* cells, const uint8_t* pbcs, const uint8_t* has_cell, double rc_max,
                  uint64_t bf_threshold, int multi, int64_t run_start, SysPlan* plans,
-                 int32_t* error_flag, cudaStream_t s);
-// counts[q * row + slot + p]; `work` must be zero on entry; cap = power of two
-// >= the largest system of the run.
-void launch_batch_count(const SysPlan* plans, const int32_t* order, int n_sys, const double* pos,
-                        int cap, const CutoffSet& cs, uint32_t* counts, int64_t row, int* work,
+                 int32_t* error_flag, cudaStream_t s, const double* sys_rc = nullptr);
+// out[s] = first edge of system s relative to the run (k == 1 rows), out[ns] = total.
+void launch_sys_bounds(const SysPlan* plans, int n_sys, const int64_t* offs, int64_t row,
+                       int64_t* out, cudaStream_t s);
+// Work items of one batched pass: (system, first atom) pairs, systems with
+// more than kBatchLargeAtoms atoms first (split into chunks, 512-thread CTAs),
+// then the smaller ones (one item each, 256-thread CTAs), each group largest
+// first.  cap_* = power of two >= the largest system of the group.
+constexpr int kBatchLargeAtoms = 512;
+struct BatchItems {
+  const int2* items = nullptr;  // device: [n_large | n_small]
+  int n_large = 0, n_small = 0;
+  int cap_large = 32, cap_small = 32;
+};
+// Host: builds the item list (upload it and set w.items before launching).
+void plan_batch_items(const int64_t* sizes, int n_sys, std::vector<int2>& items, BatchItems& w);
+// counts[q * row + slot + p]; work2[0..1] must be zero on entry.
+void launch_batch_count(const SysPlan* plans, const BatchItems& w, const double* pos,
+                        const CutoffSet& cs, uint32_t* counts, int64_t row, int* work2,
                         cudaStream_t s);
-void launch_batch_emit(const SysPlan* plans, const int32_t* order, int n_sys, const double* pos,
-                       int cap, const CutoffSet& cs, const int64_t* offs, int64_t row,
-                       const EmitTargets& t, int* work, cudaStream_t s);
+void launch_batch_emit(const SysPlan* plans, const BatchItems& w, const double* pos,
+                       const CutoffSet& cs, const int64_t* offs, int64_t row,
+                       const EmitTargets& t, int* work2, cudaStream_t s);
 
 // Sets the dynamic shared-memory limit of a kernel once per device.
 void ensure_smem_attr(const void* func, int bytes);
