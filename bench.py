@@ -59,7 +59,77 @@ def parse():
     ap.add_argument("--no-extra", action="store_true", help="headline workload only")
     ap.add_argument("--rc", type=float, default=6.0,
                     help="cutoff of the timed workload (6.0 = headline; 14.0 for profiling)")
+    ap.add_argument("--case", default=None, choices=sorted(CASES),
+                    help="run only this workload --steps times after --warmup (for profilers; "
+                         "prints one summary line, not the bench JSON)")
     return ap.parse_args()
+
+
+def _case_device(rc):
+    def run(nl, torch, steps, warmup):
+        pos, rows = headline_system()
+        dt = DeviceTimer(nl, torch, pos, rows, rc)
+        ms, edges, launches = dt.run(steps, warmup)
+        return {"edges_per_step": edges // steps, "ms_per_step": ms / steps, "launches": launches}
+    return run
+
+
+def _case_batch(nl, torch, steps, warmup):
+    from neighborlist_rs import workloads as W
+
+    pb, bb, cb = W.concat_batch(W.uneven_batch())
+    for _ in range(warmup):
+        nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r = nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0)
+    return {"edges": int(r["edge_index"].shape[1]), "ms_per_call": 1e3 * (time.perf_counter() - t0) / steps}
+
+
+def _case_served(nl, torch, steps, warmup):
+    from neighborlist_rs import workloads as W
+    from neighborlist_rs.serving import Server
+
+    reqs = [(None if s.cell_rows is None else nl.PyCell(s.cell_rows.T.tolist()), s.positions,
+             s.cutoff) for s in W.request_stream(1024, seed=21, n_range=(16, 2048))]
+    with Server(hbm_budget_bytes=40 << 30, workers=2) as srv:
+        for _ in range(warmup):
+            run_stream_raw(srv, reqs)
+        for _ in range(steps):
+            r = run_stream_raw(srv, reqs)
+    return r
+
+
+def _case_multi(nl, torch, steps, warmup):
+    from neighborlist_rs import workloads as W
+
+    p3, r3 = W.triclinic_uniform()
+    cell = nl.PyCell(r3.T.tolist())
+    for _ in range(warmup):
+        nl.build_neighborlists_multi(cell, p3, [5.0, 6.0, 12.0])
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r = nl.build_neighborlists_multi(cell, p3, [5.0, 6.0, 12.0])
+    return {"edges": sum(int(v["edge_index"].shape[1]) for v in r.values()),
+            "ms_per_call": 1e3 * (time.perf_counter() - t0) / steps}
+
+
+CASES = {
+    "cluster_liquid_rc6": _case_device(6.0),
+    "cluster_liquid_rc14": _case_device(14.0),
+    "uneven_batch_4096": _case_batch,
+    "served_small_mix_1024": _case_served,
+    "triclinic_multi_20k": _case_multi,
+}
+
+
+def run_case(args):
+    import torch
+
+    import neighborlist_rs as nl
+
+    out = CASES[args.case](nl, torch, args.steps, args.warmup)
+    print(json.dumps({"case": args.case, **out}), flush=True)
 
 
 # ---------------------------------------------------------------- distributed
@@ -271,21 +341,25 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     h, pbc = rows.T, [True] * 3
     for _ in range(args.warmup):
-        oracle.search_single(pos, h, pbc, 6.0, nthreads=threads)
+        oracle.search_single(pos, h, pbc, args.rc, nthreads=threads)
     t = 0.0
     m = 0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        ei, _ = oracle.search_single(pos, h, pbc, 6.0, nthreads=threads)
+        ei, _ = oracle.search_single(pos, h, pbc, args.rc, nthreads=threads)
         t += time.perf_counter() - t0
         m = ei.shape[1]
     value = m * args.steps / t
+    metric, workload = METRIC, WORKLOAD
+    if args.rc != 6.0:
+        metric = METRIC.replace("rc=6", f"rc={args.rc:g}")
+        workload = WORKLOAD.replace("rc=6.0", f"rc={args.rc:g}")
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "impl": "reference", "metric": metric, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "edges_per_step": m, "parallelism": "host threads"},
+        "config": {"workload": workload, "edges_per_step": m, "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{args.steps} full builds of the workload (C++ restatement "
                                    "of the reference rayon count/fill path; the Rust crate "
@@ -318,12 +392,17 @@ def run_b200(args):
     # per-phase CUDA-event times -> roofline of the dominant kernel
     ph = dt.phases(max(5, args.steps // 3))
     peak, peak_kind = peaks()
-    bytes_emit = 28 * m_step + 48 * n      # edge_index + shift writes; sorted SoA + offsets read
-    bytes_count = 44 * n                   # sorted SoA read, counts written
+    # Algorithmic bytes per launch: emit writes the 28 B/edge output and reads
+    # the sorted SoA + per-(atom, cell) offsets once; count reads the sorted
+    # FP32 coordinates and writes one count per (atom, stencil cell).
+    cells = 27  # stencil cells of this grid (n_search = 1 on every axis)
+    bytes_emit = 28 * m_step + 48 * n
+    bytes_count = 16 * n + 4 * cells * n
     dominant = "emit" if ph["emit"] >= ph["count"] else "count"
     alg = bytes_emit if dominant == "emit" else bytes_count
     achieved = alg / (ph[dominant] * 1e-3) / 1e9
-    kernel_name = {"emit": "k_grid_emit", "count": "k_grid_count"}[dominant]
+    kernel_name = {"emit": "k_pair_tasks<1> (emit pass)",
+                   "count": "k_pair_tasks<0> (count pass)"}[dominant]
 
     # e2e through the reference-facing call (host buffers)
     nl.set_stream(None)
@@ -568,7 +647,9 @@ def served_measurements(nl):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.case:
+        run_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)
