@@ -137,6 +137,34 @@ int64_t nlb_kernel_launches(void);
 void nlb_profile(int enable);
 int64_t nlb_profile_read(double* ms);
 
+/* ---- Output options (asked for by the reference's spec.md:100-108 and
+ * RUST_API.md:89-90, not implemented by the reference). ----
+ * nlb_build_ex: the nlb_build search, then on the device:
+ *   NLB_DIRECTED   the M half edges followed by their reverses (j, i, -S):
+ *                  2M edges ("double the edges and negate the shifts");
+ *   NLB_VECTORS    d = (r_j - r_i) + H.S per edge, float64 x3 (component k
+ *                  evaluated as (r_j,k - r_i,k) + ((H[k][0] S0 + H[k][1] S1)
+ *                  + H[k][2] S2); r_j - r_i when cell is NULL); reverses get -d;
+ *   NLB_DISTANCES  |d| = sqrt((d0^2 + d1^2) + d2^2), correctly rounded.
+ * Arrays not asked for are NULL.  Free with nlb_result_ex_free.
+ * nlb_build_device_ex: device positions in, device pointers into the calling
+ * thread's workspace out (valid until its next build call). */
+#define NLB_DIRECTED 1
+#define NLB_VECTORS 2
+#define NLB_DISTANCES 4
+typedef struct nlb_result_ex {
+  int64_t n_edges;     /* M, or 2M when directed */
+  int64_t* edge_index; /* 2 * n_edges int64: sources then destinations */
+  int32_t* shift;      /* 3 * n_edges int32 */
+  double* vectors;     /* 3 * n_edges float64, or NULL */
+  double* distances;   /* n_edges float64, or NULL */
+} nlb_result_ex;
+int nlb_build_ex(const double* positions, int64_t n_atoms, double cutoff, const double* cell,
+                 const uint8_t* pbc, int flags, nlb_result_ex* out);
+int nlb_build_device_ex(const double* d_positions, int64_t n_atoms, double cutoff,
+                        const double* cell, const uint8_t* pbc, int flags, nlb_result_ex* out);
+void nlb_result_ex_free(nlb_result_ex* r);
+
 /* ---- Build without allocating (no counterpart in the reference). ----
  * For callers that must not allocate GPU memory when they ask for a list:
  * processes whose HBM is held by a framework's caching allocator, code that

@@ -711,6 +711,164 @@ Status run_single(const double* pos, int64_t n, const double* cell9, const uint8
   return st;
 }
 
+// One system, one cutoff: the half list on the device ([src | dst] *ei, *sh,
+// *m edges), on c.stream.  pos_host (optional) serves the auto-box planner;
+// without it the bounds come from the device positions.
+Status half_list_device(Ctx& c, const double* pos_host, const double* d_pos, int64_t n,
+                        const double* cell9, const uint8_t* pbc, double cutoff, int64_t** ei,
+                        int32_t** sh, int64_t* m) {
+  double bounds[6];
+  const double* bptr = nullptr;
+  if (!cell9 && !pos_host) {
+    double* d_b = static_cast<double*>(c.raw(kSlotBatch0 + 31, sizeof(double) * 6));
+    if (!d_b) return fail(NLB_ERR_NOMEM, "device allocation failed");
+    launch_bounds(d_pos, n, d_b, c.stream);
+    cudaError_t e = cudaMemcpyAsync(bounds, d_b, sizeof(bounds), cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess) return cuda_fail(e, "bounds");
+    bptr = bounds;
+  }
+  const bool pb[3] = {pbc ? pbc[0] != 0 : true, pbc ? pbc[1] != 0 : true,
+                      pbc ? pbc[2] != 0 : true};
+  SystemPlan sp;
+  std::vector<double> cs(1, cutoff);
+  Status st = plan_system(pos_host, n, cell9, pb, cs, false, false, sp, bptr);
+  if (!st.ok()) return st;
+  if (fast_eligible(sp)) {
+    st = run_fast(c, sp, d_pos, m);
+    if (!st.ok()) return st;
+    *ei = sp.out_src;
+    *sh = sp.out_sh;
+    return Status{NLB_OK};
+  }
+  st = count_system(c, sp, d_pos);
+  if (!st.ok()) return st;
+  DevLists L;
+  st = device_outputs(c, sp.m, L);
+  if (!st.ok()) return st;
+  const int64_t zero = 0;
+  st = emit_system(c, sp, d_pos, L, &zero, 0);
+  if (!st.ok()) return st;
+  *m = sp.m[0];
+  *ei = L.src[0];
+  *sh = L.sh[0];
+  return Status{NLB_OK};
+}
+
+// Output options applied to a device half list; results in workspace slots
+// (or the half list itself when nothing changes it).
+Status apply_extras(Ctx& c, const double* d_pos, const double* cell9, int flags, int64_t* ei,
+                    int32_t* sh, int64_t m, nlb_result_ex* out) {
+  const bool directed = (flags & NLB_DIRECTED) != 0;
+  const int64_t mo = directed ? 2 * m : m;
+  out->n_edges = mo;
+  out->edge_index = ei;
+  out->shift = sh;
+  out->vectors = nullptr;
+  out->distances = nullptr;
+  if (directed) {
+    out->edge_index = slot<int64_t>(c, kSlotBatch0 + 20, 2 * (size_t)mo);
+    out->shift = slot<int32_t>(c, kSlotBatch0 + 21, 3 * (size_t)mo);
+    if (!out->edge_index || !out->shift) return fail(NLB_ERR_NOMEM, "device allocation failed");
+  }
+  if (flags & NLB_VECTORS) {
+    out->vectors = slot<double>(c, kSlotBatch0 + 22, 3 * (size_t)mo);
+    if (!out->vectors) return fail(NLB_ERR_NOMEM, "device allocation failed");
+  }
+  if (flags & NLB_DISTANCES) {
+    out->distances = slot<double>(c, kSlotBatch0 + 23, (size_t)mo);
+    if (!out->distances) return fail(NLB_ERR_NOMEM, "device allocation failed");
+  }
+  if (!directed && !out->vectors && !out->distances) return Status{NLB_OK};
+  EdgeExtrasCell cell{};
+  if (cell9) {
+    for (int k = 0; k < 9; ++k) cell.h[k] = cell9[k];
+    cell.has_cell = 1;
+  }
+  launch_edge_extras(d_pos, cell, ei, sh, m, directed ? 1 : 0, directed ? out->edge_index : nullptr,
+                     directed ? out->shift : nullptr, out->vectors, out->distances, c.stream);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "edge extras launch");
+  return Status{NLB_OK};
+}
+
+bool extras_flags_valid(int flags) {
+  return (flags & ~(NLB_DIRECTED | NLB_VECTORS | NLB_DISTANCES)) == 0;
+}
+
+// nlb_build_ex / nlb_build_device_ex: d_pos_in == nullptr means host
+// positions (uploaded here) and pinned host results.
+Status run_single_ex(const double* pos, const double* d_pos_in, int64_t n, const double* cell9,
+                     const uint8_t* pbc, double cutoff, int flags, nlb_result_ex* out) {
+  std::memset(out, 0, sizeof(*out));
+  if (!extras_flags_valid(flags)) return fail(NLB_ERR_VALUE, "unknown output option flags");
+  if (!cutoffs_valid(&cutoff, 1)) return fail(NLB_ERR_VALUE, "Cutoff must be positive and finite");
+  if (n < 0) return fail(NLB_ERR_VALUE, "Positions must be (N, 3)");
+  const bool host = d_pos_in == nullptr;
+  if (n > 0 && host && !pos) return fail(NLB_ERR_VALUE, "positions is NULL");
+  Ctx* c = nullptr;
+  Status st = get_ctx(&c);
+  if (!st.ok()) return st;
+  int64_t* ei = nullptr;
+  int32_t* sh = nullptr;
+  int64_t m = 0;
+  const double* d_pos = d_pos_in;
+  if (n > 0) {
+    if (host) {
+      double* up = nullptr;
+      st = upload_positions(*c, pos, n, &up);
+      if (!st.ok()) return st;
+      d_pos = up;
+    }
+    st = half_list_device(*c, host ? pos : nullptr, d_pos, n, cell9, pbc, cutoff, &ei, &sh, &m);
+    if (!st.ok()) return st;
+  }
+  nlb_result_ex dev;
+  st = apply_extras(*c, d_pos, cell9, flags, ei, sh, m, &dev);
+  if (!st.ok()) return st;
+  if (!host) {
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "edge extras");
+    if (c->prof) c->harvest();
+    *out = dev;
+    return Status{NLB_OK};
+  }
+  // Pinned host results.
+  const int64_t mo = dev.n_edges;
+  const size_t cnt = (size_t)std::max<int64_t>(mo, 1);
+  out->n_edges = mo;
+  out->edge_index = static_cast<int64_t*>(pinned_alloc(16 * cnt));
+  out->shift = static_cast<int32_t*>(pinned_alloc(12 * cnt));
+  if (flags & NLB_VECTORS) out->vectors = static_cast<double*>(pinned_alloc(24 * cnt));
+  if (flags & NLB_DISTANCES) out->distances = static_cast<double*>(pinned_alloc(8 * cnt));
+  if (!out->edge_index || !out->shift || ((flags & NLB_VECTORS) && !out->vectors) ||
+      ((flags & NLB_DISTANCES) && !out->distances)) {
+    nlb_result_ex_free(out);
+    return fail(NLB_ERR_NOMEM, "pinned host allocation failed");
+  }
+  cudaError_t e = cudaSuccess;
+  if (mo > 0) {
+    e = cudaMemcpyAsync(out->edge_index, dev.edge_index, 16 * (size_t)mo, cudaMemcpyDeviceToHost,
+                        c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out->shift, dev.shift, 12 * (size_t)mo, cudaMemcpyDeviceToHost,
+                          c->stream);
+    if (e == cudaSuccess && out->vectors)
+      e = cudaMemcpyAsync(out->vectors, dev.vectors, 24 * (size_t)mo, cudaMemcpyDeviceToHost,
+                          c->stream);
+    if (e == cudaSuccess && out->distances)
+      e = cudaMemcpyAsync(out->distances, dev.distances, 8 * (size_t)mo,
+                          cudaMemcpyDeviceToHost, c->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    nlb_result_ex_free(out);
+    return cuda_fail(e, "result copy");
+  }
+  if (c->prof) c->harvest();
+  return Status{NLB_OK};
+}
+
 // One system, one cutoff, device in / device out (nlb_build_device).
 Status run_single_device(const double* d_pos, int64_t n, const double* cell9, const uint8_t* pbc,
                          double cutoff, nlb_device_result* out) {
@@ -810,6 +968,35 @@ int nlb_build_batch_multi(const double* positions, int64_t n_atoms, const int32_
   return run_batch(positions, n_atoms, batch, n_batch, cutoffs, n_cutoffs, cells, pbcs, has_cell,
                    n_cells, disjoint != 0, true, outs)
       .code;
+}
+
+int nlb_build_ex(const double* positions, int64_t n_atoms, double cutoff, const double* cell,
+                 const uint8_t* pbc, int flags, nlb_result_ex* out) {
+  if (!out) return fail(NLB_ERR_VALUE, "out is NULL").code;
+  return run_single_ex(positions, nullptr, n_atoms, cell, pbc, cutoff, flags, out).code;
+}
+
+int nlb_build_device_ex(const double* d_positions, int64_t n_atoms, double cutoff,
+                        const double* cell, const uint8_t* pbc, int flags, nlb_result_ex* out) {
+  if (!out) return fail(NLB_ERR_VALUE, "out is NULL").code;
+  if (!d_positions && n_atoms > 0) {
+    std::memset(out, 0, sizeof(*out));
+    return fail(NLB_ERR_VALUE, "positions is NULL").code;
+  }
+  // A non-null placeholder selects the device-result path for empty input.
+  static const double kNone = 0.0;
+  return run_single_ex(nullptr, d_positions ? d_positions : &kNone, n_atoms, cell, pbc, cutoff,
+                       flags, out)
+      .code;
+}
+
+void nlb_result_ex_free(nlb_result_ex* r) {
+  if (!r) return;
+  pinned_release(r->edge_index);
+  pinned_release(r->shift);
+  pinned_release(r->vectors);
+  pinned_release(r->distances);
+  std::memset(r, 0, sizeof(*r));
 }
 
 void nlb_result_free(nlb_result* r) {

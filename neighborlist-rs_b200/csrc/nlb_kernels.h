@@ -194,4 +194,15 @@ void note_launches(int n);
 // reference's `<` / `>` scan starting from +/-inf).
 void launch_bounds(const double* pos, int64_t n, double* out, cudaStream_t s);
 
+// Output options on a device half list ([src | dst] ei, shifts sh, m edges):
+// directed list, displacement vectors, distances (k_extras.cu).  Outputs
+// that are not wanted are NULL; with directed == 0 ei_out/sh_out may be NULL.
+struct EdgeExtrasCell {
+  double h[9];       // row-major H (columns = lattice vectors)
+  int32_t has_cell;  // 0: no H term (vectors are r_j - r_i)
+};
+void launch_edge_extras(const double* pos, const EdgeExtrasCell& cell, const int64_t* ei,
+                        const int32_t* sh, int64_t m, int directed, int64_t* ei_out,
+                        int32_t* sh_out, double* vec, double* dist, cudaStream_t s);
+
 }  // namespace nlb

@@ -445,12 +445,17 @@ def build_device_raw(cell, positions_ptr: int, n_atoms: int, cutoff: float):
     return int(r.n_edges), r.edge_index, r.shift
 
 
-def build_neighborlists_torch(cell, positions, cutoff):
+def build_neighborlists_torch(cell, positions, cutoff, directed=False, vectors=False,
+                              distances=False):
     """GPU-resident variant of build_neighborlists for torch pipelines:
     ``positions`` is a CUDA float64 tensor (N, 3); returns
     {"edge_index": int64 (2, M), "shift": int32 (M, 3)} as CUDA tensors on the
     same device, produced on the current torch stream (no host round trip
-    for the edge arrays)."""
+    for the edge arrays).  directed / vectors / distances as in
+    build_neighborlists_ex (adds "vectors" float64 (M, 3) and "distances"
+    float64 (M,))."""
+    if directed or vectors or distances:
+        return _torch_ex(cell, positions, cutoff, directed, vectors, distances)
     import torch
 
     if not (isinstance(positions, torch.Tensor) and positions.is_cuda
@@ -484,6 +489,98 @@ _lib.nlb_copy_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size
                                  ctypes.c_void_p]
 
 
+# ---------------------------------------------------------------- output options
+
+class _ResultEx(ctypes.Structure):
+    _fields_ = [("n_edges", ctypes.c_int64),
+                ("edge_index", ctypes.c_void_p),
+                ("shift", ctypes.c_void_p),
+                ("vectors", ctypes.c_void_p),
+                ("distances", ctypes.c_void_p)]
+
+
+_NLB_DIRECTED, _NLB_VECTORS, _NLB_DISTANCES = 1, 2, 4
+_lib.nlb_build_ex.argtypes = [_dp, ctypes.c_int64, ctypes.c_double, _dp, _u8p, ctypes.c_int,
+                              ctypes.POINTER(_ResultEx)]
+_lib.nlb_build_device_ex.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, _dp,
+                                     _u8p, ctypes.c_int, ctypes.POINTER(_ResultEx)]
+_lib.nlb_result_ex_free.argtypes = [ctypes.POINTER(_ResultEx)]
+
+
+def _ex_flags(directed, vectors, distances) -> int:
+    return ((_NLB_DIRECTED if directed else 0) | (_NLB_VECTORS if vectors else 0)
+            | (_NLB_DISTANCES if distances else 0))
+
+
+def build_neighborlists_ex(cell, positions, cutoff, directed=False, vectors=False,
+                           distances=False):
+    """build_neighborlists with the output options of the reference's
+    specification (spec.md:100-108, RUST_API.md:89-90), computed on the GPU:
+
+    * directed: the half list followed by every edge reversed, (j, i, -S)
+      ("double the edges and negate the shifts");
+    * vectors: "vectors" float64 (M, 3), d = (r_j - r_i) + H S (H columns =
+      lattice vectors; r_j - r_i without a cell); reversed edges get -d;
+    * distances: "distances" float64 (M,), |d| (correctly rounded sqrt).
+    """
+    c = _check_cutoff(cutoff)
+    pos = _positions(positions)
+    n = pos.shape[0]
+    h, pb = _cell_args(cell)
+    r = _ResultEx()
+    _check(_lib.nlb_build_ex(pos.ctypes.data_as(_dp), n, c, h, pb,
+                             _ex_flags(directed, vectors, distances), ctypes.byref(r)))
+    m = int(r.n_edges)
+    out = {"edge_index": _arr(r.edge_index, 2 * m, ctypes.c_int64, np.int64).reshape(2, m),
+           "shift": _arr(r.shift, 3 * m, ctypes.c_int32, np.int32).reshape(m, 3)}
+    if vectors:
+        out["vectors"] = _arr(r.vectors, 3 * m, ctypes.c_double, np.float64).reshape(m, 3)
+    if distances:
+        out["distances"] = _arr(r.distances, m, ctypes.c_double, np.float64)
+    return out
+
+
 def _cudart_copy(dst, src, nbytes, stream):
     _check(_lib.nlb_copy_device(ctypes.c_void_p(dst), ctypes.c_void_p(src), nbytes,
                                 ctypes.c_void_p(stream)))
+
+
+def _torch_ex(cell, positions, cutoff, directed, vectors, distances):
+    import torch
+
+    if not (isinstance(positions, torch.Tensor) and positions.is_cuda
+            and positions.dtype == torch.float64 and positions.dim() == 2):
+        raise TypeError("positions must be a CUDA float64 tensor of shape (N, 3)")
+    if positions.shape[1] != 3:
+        raise ValueError("Positions must be (N, 3)")
+    c = _check_cutoff(cutoff)
+    pos = positions.contiguous()
+    dev = pos.device
+    n = pos.shape[0]
+    h, pb = _cell_args(cell)
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev)
+        set_stream(stream.cuda_stream)
+        try:
+            r = _ResultEx()
+            _check(_lib.nlb_build_device_ex(ctypes.c_void_p(pos.data_ptr() if n else 0), n, c, h,
+                                            pb, _ex_flags(directed, vectors, distances),
+                                            ctypes.byref(r)))
+            m = int(r.n_edges)
+            out = {"edge_index": torch.empty((2, m), dtype=torch.int64, device=dev),
+                   "shift": torch.empty((m, 3), dtype=torch.int32, device=dev)}
+            if vectors:
+                out["vectors"] = torch.empty((m, 3), dtype=torch.float64, device=dev)
+            if distances:
+                out["distances"] = torch.empty((m,), dtype=torch.float64, device=dev)
+            if m:
+                s = stream.cuda_stream
+                _cudart_copy(out["edge_index"].data_ptr(), r.edge_index, 16 * m, s)
+                _cudart_copy(out["shift"].data_ptr(), r.shift, 12 * m, s)
+                if vectors:
+                    _cudart_copy(out["vectors"].data_ptr(), r.vectors, 24 * m, s)
+                if distances:
+                    _cudart_copy(out["distances"].data_ptr(), r.distances, 8 * m, s)
+        finally:
+            set_stream(None)
+    return out

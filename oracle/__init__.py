@@ -84,6 +84,10 @@ def lib():
                                        ctypes.c_int64, dp, u8p, u8p, ctypes.c_int64, dp,
                                        ctypes.c_int32, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(_Edges)]
+        i64p = ctypes.POINTER(ctypes.c_int64)
+        L.orc_edge_extras.argtypes = [dp, dp, i64p, i64p, ctypes.POINTER(ctypes.c_int32),
+                                      ctypes.c_int64, ctypes.c_int, i64p,
+                                      ctypes.POINTER(ctypes.c_int32), dp, dp]
         _lib = L
     return _lib
 
@@ -246,3 +250,30 @@ def cell_list(positions, h, cutoff):
                            abin.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))):
         raise RuntimeError("Cell matrix is not invertible")
     return nb, ns, parts[: p.shape[0]], abin[: p.shape[0]]
+
+
+def edge_extras(positions, h, edges, directed=False):
+    """spec.md:100-108 / RUST_API.md:89-90 output options on a half list
+    (edge_index (2, M), shift (M, 3)): returns (edge_index (2, Mo), shift
+    (Mo, 3), vectors (Mo, 3), distances (Mo,)), Mo = 2M if directed.
+    h=None: the system has no cell (vectors are r_j - r_i)."""
+    p = _pos(positions)
+    ei, sh = edges
+    m = ei.shape[1]
+    mo = 2 * m if directed else m
+    src = np.ascontiguousarray(ei[0], dtype=np.int64)
+    dst = np.ascontiguousarray(ei[1], dtype=np.int64)
+    s = np.ascontiguousarray(sh, dtype=np.int32).reshape(-1)
+    h9 = None if h is None else np.ascontiguousarray(np.asarray(h, dtype=np.float64).reshape(9))
+    ei_out = np.zeros(max(2 * mo, 1), np.int64)
+    sh_out = np.zeros(max(3 * mo, 1), np.int32)
+    vec = np.zeros(max(3 * mo, 1), np.float64)
+    dist = np.zeros(max(mo, 1), np.float64)
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    lib().orc_edge_extras(_dp(p), _dp(h9), src.ctypes.data_as(i64p), dst.ctypes.data_as(i64p),
+                          s.ctypes.data_as(i32p), m, int(bool(directed)),
+                          ei_out.ctypes.data_as(i64p), sh_out.ctypes.data_as(i32p), _dp(vec),
+                          _dp(dist))
+    return (ei_out[: 2 * mo].reshape(2, mo), sh_out[: 3 * mo].reshape(mo, 3),
+            vec[: 3 * mo].reshape(mo, 3), dist[:mo])

@@ -23,6 +23,10 @@
 //                            mic_safe, dispatch)
 //   src/batch.rs:10-290      search_batch / search_batch_multi
 //   src/config.rs:4-40       brute-force / parallel thresholds
+//   spec.md:100-108, RUST_API.md:89-90
+//                            directed list, displacement vectors, distances
+//                            (orc_edge_extras; asked for by the spec, not
+//                            implemented by the reference)
 //
 // Third-party arithmetic restated (no Cargo.lock in the reference; Cargo.toml
 // pins nalgebra ^0.34.1, wide ^1.1.1):
@@ -802,6 +806,60 @@ int orc_search_batch(const double* pos, int64_t n, const int32_t* batch, int64_t
     export_edges(all, 0, &outs[q]);
   }
   return 0;
+}
+
+// Output options beyond the reference's half list (spec.md:100-108 asks for
+// a directed option; RUST_API.md:89-90 documents it as "double the edges and
+// negate the shifts").  Half edge e = (i, j, S):
+//   vector   d = (r_j - r_i) + H.S, component k: (r_j,k - r_i,k) +
+//            ((H[k][0] S0 + H[k][1] S1) + H[k][2] S2)   (no H term when the
+//            system has no cell: d = r_j - r_i)
+//   distance sqrt((d0^2 + d1^2) + d2^2), correctly rounded
+//   directed the m half edges, then their reverses (j, i, -S, -d, same distance)
+// Outputs: ei_out [2 mo] ([src | dst]), sh_out [3 mo], vec [3 mo], dist [mo],
+// mo = directed ? 2m : m; any output may be NULL.
+void orc_edge_extras(const double* pos, const double* h9, const int64_t* ei, const int64_t* ej,
+                     const int32_t* sh, int64_t m, int directed, int64_t* ei_out,
+                     int32_t* sh_out, double* vec, double* dist) {
+  const int64_t mo = directed ? 2 * m : m;
+  for (int64_t e = 0; e < m; ++e) {
+    const int64_t i = ei[e], j = ej[e];
+    const int32_t* s = sh + 3 * e;
+    double d[3];
+    for (int k = 0; k < 3; ++k) {
+      const double rel = pos[3 * j + k] - pos[3 * i + k];
+      if (h9) {
+        const double hs = (h9[3 * k] * (double)s[0] + h9[3 * k + 1] * (double)s[1]) +
+                          h9[3 * k + 2] * (double)s[2];
+        d[k] = rel + hs;
+      } else {
+        d[k] = rel;
+      }
+    }
+    const double r = std::sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]);
+    if (ei_out) {
+      ei_out[e] = i;
+      ei_out[mo + e] = j;
+      if (directed) {
+        ei_out[m + e] = j;
+        ei_out[mo + m + e] = i;
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      if (sh_out) {
+        sh_out[3 * e + k] = s[k];
+        if (directed) sh_out[3 * (m + e) + k] = -s[k];
+      }
+      if (vec) {
+        vec[3 * e + k] = d[k];
+        if (directed) vec[3 * (m + e) + k] = -d[k];
+      }
+    }
+    if (dist) {
+      dist[e] = r;
+      if (directed) dist[m + e] = r;
+    }
+  }
 }
 
 }  // extern "C"
