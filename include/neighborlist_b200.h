@@ -165,6 +165,38 @@ int nlb_build_device_ex(const double* d_positions, int64_t n_atoms, double cutof
                         const double* cell, const uint8_t* pbc, int flags, nlb_result_ex* out);
 void nlb_result_ex_free(nlb_result_ex* r);
 
+/* ---- Verlet (skin) list manager for MD (asked for by the reference's
+ * spec.md:41-48, 64-67, 209-222 as DynamicNeighborManager; not implemented
+ * by the reference). ----
+ * nlb_verlet_create: cutoff rc, skin >= 0; the stored list is the exact half
+ *   list at rc + skin (the nlb_build search) of the reference positions.
+ * nlb_verlet_update: host positions in, host result out (free with
+ *   nlb_result_free).  Rebuilds (*rebuilt = 1) when there is no list, the
+ *   atom count, cell or pbc changed, or max_i |r_i - r_i,ref| > skin / 2;
+ *   then returns the stored edges (i, j, S) with |(r_j - r_i) + H.S| < rc for
+ *   the given positions, in stored order (the pairs a fresh nlb_build at rc
+ *   finds, as long as positions are continuous; re-wrapped atoms force a
+ *   rebuild).  One synchronisation per update without a rebuild.
+ * nlb_verlet_update_device: device positions in; the result arrays are
+ *   device pointers owned by the manager, valid until its next update.
+ * nlb_verlet_needs_rebuild: *needs and the current max displacement (+inf
+ *   when the next update rebuilds anyway); positions_on_device selects the
+ *   pointer kind.
+ * nlb_verlet_stats: updates, rebuilds, stored edges, edges last returned.
+ * A manager is used by one thread at a time (calls are serialised). */
+typedef struct nlb_verlet nlb_verlet;
+nlb_verlet* nlb_verlet_create(double cutoff, double skin);
+int nlb_verlet_update(nlb_verlet* v, const double* positions, int64_t n_atoms, const double* cell,
+                      const uint8_t* pbc, int* rebuilt, nlb_result* out);
+int nlb_verlet_update_device(nlb_verlet* v, const double* d_positions, int64_t n_atoms,
+                             const double* cell, const uint8_t* pbc, int* rebuilt,
+                             nlb_device_result* out);
+int nlb_verlet_needs_rebuild(nlb_verlet* v, const double* positions, int64_t n_atoms,
+                             const double* cell, const uint8_t* pbc, int positions_on_device,
+                             int* needs, double* max_displacement);
+void nlb_verlet_stats(nlb_verlet* v, int64_t* stats);
+void nlb_verlet_destroy(nlb_verlet* v);
+
 /* ---- Build without allocating (no counterpart in the reference). ----
  * For callers that must not allocate GPU memory when they ask for a list:
  * processes whose HBM is held by a framework's caching allocator, code that
