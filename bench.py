@@ -502,7 +502,66 @@ def extra_measurements(nl, torch, args):
         "plain_per_system_loop_systems_per_s": sample / tp,
         "atoms": int(pb.shape[0]), "edges": mb}
     out["served"] = served_measurements(nl)
+    out["output_options_rc6"] = output_option_measurements(nl, torch)
+    out["verlet_md_rc6"] = verlet_measurements(nl, torch)
     return out
+
+
+def _median_device_call(torch, fn, reps=20, warmup=3):
+    """Median wall time (s) of fn() with a device sync after each call."""
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts)
+
+
+def output_option_measurements(nl, torch):
+    """Headline system through build_neighborlists_torch (device in, device
+    out): half list vs directed list with vectors and distances."""
+    pos, rows = headline_system()
+    cell = nl.PyCell(rows.T.tolist())
+    dpos = torch.from_numpy(pos).cuda()
+    t_half = _median_device_call(torch, lambda: nl.build_neighborlists_torch(cell, dpos, 6.0))
+    r = nl.build_neighborlists_torch(cell, dpos, 6.0, directed=True, vectors=True,
+                                     distances=True)
+    m = int(r["edge_index"].shape[1])
+    t_full = _median_device_call(torch, lambda: nl.build_neighborlists_torch(
+        cell, dpos, 6.0, directed=True, vectors=True, distances=True))
+    return {"half_list_ms": 1e3 * t_half, "directed_vectors_distances_ms": 1e3 * t_full,
+            "directed_edges": m, "directed_edges_per_s": m / t_full,
+            "bytes_out_per_edge": 28 + 24 + 8}
+
+
+def verlet_measurements(nl, torch):
+    """MD-style use of the headline system: Verlet list at rc 6 with a 1 A
+    skin, positions moved by 0.01 A per step (no rebuild inside the sample),
+    device positions in, device lists out; against a fresh build per step."""
+    from neighborlist_rs.verlet import VerletList
+
+    pos, rows = headline_system()
+    cell = nl.PyCell(rows.T.tolist())
+    rng = np.random.default_rng(31)
+    steps = [torch.from_numpy(pos + rng.normal(0.0, 0.01 / 3 ** 0.5, pos.shape) * (k + 1) / 20)
+             .cuda() for k in range(20)]
+    with VerletList(6.0, 1.0) as vl:
+        vl.update(cell, steps[0])
+        k = [0]
+
+        def one():
+            vl.update(cell, steps[k[0] % 20])
+            k[0] += 1
+        t_upd = _median_device_call(torch, one, reps=40, warmup=5)
+        st = vl.stats()
+    t_fresh = _median_device_call(torch, lambda: nl.build_neighborlists_torch(cell, steps[5], 6.0))
+    return {"update_ms": 1e3 * t_upd, "fresh_build_ms": 1e3 * t_fresh,
+            "stored_edges_rc7": st["stored_edges"], "edges_rc6": st["last_edges"],
+            "rebuilds": st["rebuilds"], "updates": st["updates"]}
 
 
 def run_stream(srv, reqs, rate, seed=0):

@@ -323,3 +323,19 @@ def test_torch_device_api(nl, oracle):
                      "shift": r["shift"].cpu().numpy()}, ref, f"torch call {it}")
     r0 = nl.build_neighborlists_torch(cell, d[:0], 6.0)
     assert r0["edge_index"].shape == (2, 0)
+
+
+def test_far_images_take_full_transfer(nl, oracle):
+    """Host-bound lists travel in a compact form whose shifts hold
+    [-511, 511]; atoms hundreds of cells away from the box give larger
+    shifts, so that call falls back to the full form -- same result."""
+    from neighborlist_rs import workloads as W
+
+    pos, rows = W.cluster_liquid(n_clusters=200, box=26.0, seed=5)
+    far = pos.copy()
+    far[:40] += rows[0] * 700.0 + rows[2] * -600.0   # 700 / -600 cell lengths away
+    for p in (pos, far):
+        got = nl.build_neighborlists(nl.PyCell(rows.T.tolist()), p, 6.0)
+        ref = oracle.search_single(p, rows.T, [True] * 3, 6.0, nthreads=8)
+        assert_same(got, ref, "far images" if p is far else "near")
+    assert np.abs(got["shift"]).max() > 511
