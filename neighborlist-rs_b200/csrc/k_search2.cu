@@ -31,6 +31,10 @@ namespace nlb {
 namespace {
 
 constexpr int kPairWarps = 8;  // warps per CTA
+// Emit pass: hits of one task staged per warp before the warp writes them out
+// (dynamic shared memory, kPairWarps x kStageCap words).
+constexpr int kStageCap = 1536;
+constexpr size_t kEmitSmem = sizeof(uint32_t) * kPairWarps * kStageCap;
 
 struct CellDesc {
   int32_t b0, b1;  // candidate slots
@@ -166,6 +170,12 @@ __global__ void __launch_bounds__(kPairWarps * 32)
   __shared__ float4 stage_q[kPairWarps][32];
   __shared__ SlotMeta stage_m[kPairWarps][32];
   __shared__ char4 stencil[kPairMaxCells];  // (dx, dy, dz) of each stencil cell, x outer
+  // Emit pass: per warp, each lane's first output slot minus its stage offset,
+  // each lane's atom meta, and the staged hits (lane << 16 | candidate offset
+  // in the cell) of the current task.
+  __shared__ int64_t lane_base[EMIT ? kPairWarps : 1][32];
+  __shared__ SlotMeta lane_meta[EMIT ? kPairWarps : 1][32];
+  extern __shared__ uint32_t stage_hits[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   {
     const int32_t ny = 2 * g.ns[1] + 1, nz = 2 * g.ns[2] + 1;
@@ -208,9 +218,73 @@ __global__ void __launch_bounds__(kPairWarps * 32)
         const int32_t s0 = (int32_t)(pw << 22) >> 22;
         const int32_t s1 = (int32_t)(pw << 12) >> 22;
         const int32_t s2 = (int32_t)(pw << 2) >> 22;
-        int64_t slot = mine ? t.base[0] + (offs[(int64_t)p * n_cells + c] - off0) : 0;
+        int64_t slot = 0;
+        int32_t cnt = 0;
         SlotMeta mi{};
-        if (mine) mi = b.meta[p];
+        if (mine) {
+          const int64_t idx = (int64_t)p * n_cells + c;
+          const int64_t o0 = offs[idx];
+          slot = t.base[0] + (o0 - off0);
+          cnt = (int32_t)(offs[idx + 1] - o0);
+          mi = b.meta[p];
+        }
+        // Stage the task's hits (lane's hits at [pre, pre + cnt)), then write
+        // them with the whole warp in stage order: each lane's (atom, cell)
+        // run is contiguous in the output, so consecutive threads store to
+        // consecutive slots instead of 32 lanes storing to 32 runs.
+        int32_t pre = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int32_t y = __shfl_up_sync(0xffffffffu, pre, o);
+          if (lane >= o) pre += y;
+        }
+        const int32_t total = __shfl_sync(0xffffffffu, pre, 31);
+        pre -= cnt;
+        if (total <= kStageCap && h1 - h0 <= 65536) {
+          uint32_t* st = stage_hits + warp * kStageCap;
+          lane_base[warp][lane] = slot - pre;
+          lane_meta[warp][lane] = mi;
+          int32_t r = pre;
+          const int32_t r_end = pre + cnt;  // the lane's own stage range
+          for (int32_t jb = h0; jb < h1; jb += 32) {
+            uint32_t hits = mine ? b.masks[(int64_t)hdr.x + (jb - h0) + lane] : 0u;
+            while (hits) {
+              const int jj = __ffs(hits) - 1;
+              hits &= hits - 1;
+              if (r < r_end) st[r] = ((uint32_t)lane << 16) | (uint32_t)(jb - h0 + jj);
+              ++r;
+            }
+          }
+          __syncwarp();
+          // Four waves at a time: their candidate gathers are in flight
+          // together before any of their stores.
+          for (int32_t k0 = lane; k0 < total; k0 += 4 * 32) {
+            uint32_t v[4];
+            SlotMeta mj[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int32_t k = k0 + 32 * u;
+              v[u] = k < total ? st[k] : 0u;
+              if (k < total) mj[u] = b.meta[h0 + (int32_t)(v[u] & 0xffffu)];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int32_t k = k0 + 32 * u;
+              if (k >= total) break;
+              const int l = (int)(v[u] >> 16);
+              const SlotMeta ml = lane_meta[warp][l];
+              const int64_t e = lane_base[warp][l] + k;
+              t.src[0][e] = (int64_t)ml.orig + t.index_offset;
+              dst0[e] = (int64_t)mj[u].orig + t.index_offset;
+              int32_t* sp = t.sh[0] + 3 * e;
+              sp[0] = (mj[u].sx - ml.sx) + s0;
+              sp[1] = (mj[u].sy - ml.sy) + s1;
+              sp[2] = (mj[u].sz - ml.sz) + s2;
+            }
+          }
+          __syncwarp();
+          continue;
+        }
         for (int32_t jb = h0; jb < h1; jb += 32) {
           uint32_t hits = mine ? b.masks[(int64_t)hdr.x + (jb - h0) + lane] : 0u;
           if (!__any_sync(0xffffffffu, hits != 0)) continue;
@@ -356,11 +430,11 @@ __global__ void __launch_bounds__(kPairWarps * 32)
   if (!EMIT && blockIdx.x == 0 && threadIdx.x == 0) counts[n * (int64_t)n_cells] = 0;
 }
 
-int pair_grid(const void* func) {
+int pair_grid(const void* func, size_t smem) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kPairWarps * 32, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kPairWarps * 32, smem);
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
@@ -400,7 +474,7 @@ void launch_pair_count(const GridParams& g, const GridBuffers& b, int64_t n,
                        const GuardBand& band, uint32_t* counts, cudaStream_t s) {
   EmitTargets t{};
   const int32_t cells = stencil_cells(g);
-  k_pair_tasks<false><<<pair_grid((const void*)k_pair_tasks<false>), kPairWarps * 32, 0, s>>>(
+  k_pair_tasks<false><<<pair_grid((const void*)k_pair_tasks<false>, 0), kPairWarps * 32, 0, s>>>(
       g, b, n, cells, band, counts, nullptr, t);
   note_launches(1);
 }
@@ -409,8 +483,9 @@ void launch_pair_emit(const GridParams& g, const GridBuffers& b, int64_t n,
                       const GuardBand& band, const int64_t* offs, const EmitTargets& t,
                       cudaStream_t s) {
   const int32_t cells = stencil_cells(g);
-  k_pair_tasks<true><<<pair_grid((const void*)k_pair_tasks<true>), kPairWarps * 32, 0, s>>>(
-      g, b, n, cells, band, nullptr, offs, t);
+  ensure_smem_attr((const void*)k_pair_tasks<true>, (int)kEmitSmem);
+  k_pair_tasks<true><<<pair_grid((const void*)k_pair_tasks<true>, kEmitSmem), kPairWarps * 32,
+                       kEmitSmem, s>>>(g, b, n, cells, band, nullptr, offs, t);
   note_launches(1);
 }
 

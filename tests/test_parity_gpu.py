@@ -339,3 +339,18 @@ def test_far_images_take_full_transfer(nl, oracle):
         ref = oracle.search_single(p, rows.T, [True] * 3, 6.0, nthreads=8)
         assert_same(got, ref, "far images" if p is far else "near")
     assert np.abs(got["shift"]).max() > 511
+
+
+@pytest.mark.parametrize("rc", [8.0, 12.0])
+def test_dense_system_emit_paths(nl, oracle, rc):
+    """A dense liquid where a (32-atom group, stencil cell) task has a few
+    hundred (rc 8) to a few thousand (rc 12) hits: the emit pass stages small
+    tasks in shared memory and writes large ones lane by lane; both give the
+    oracle's edges in the oracle's order."""
+    rng = np.random.default_rng(17)
+    box = 36.0
+    pos = rng.random((20000, 3)) * box
+    h = np.eye(3) * box
+    got = nl.build_neighborlists(nl.PyCell(h.tolist()), pos, rc)
+    ref = oracle.search_single(pos, h, PBC3, rc, nthreads=16)
+    assert_same(got, ref, f"dense liquid rc {rc}")
