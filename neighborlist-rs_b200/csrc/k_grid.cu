@@ -65,17 +65,62 @@ __global__ void k_rank_table(GridParams g, int32_t* __restrict__ rank_of_bin) {
   rank_of_bin[lin] = (int32_t)morton_rank(c, g.nb);
 }
 
-__global__ void k_prep(GridParams g, const double* __restrict__ pos, int64_t n,
-                       const int32_t* __restrict__ rank_of_bin, uint64_t* __restrict__ key,
-                       int32_t* __restrict__ rank, int32_t* __restrict__ bin_count) {
+constexpr int kPrepThreads = 256;
+
+// Exclusive scan of the bin histogram by one CTA (kPrepThreads threads):
+// bin_start[b] = sum of counts below b, bin_start[nb] = total.
+__device__ void cta_bin_scan(const int32_t* __restrict__ bin_count, int64_t nb,
+                             int64_t* __restrict__ bin_start) {
+  __shared__ int64_t warp_tot[kPrepThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t per = (nb + kPrepThreads - 1) / kPrepThreads;
+  const int64_t b0 = tid * per < nb ? tid * per : nb;
+  const int64_t b1 = b0 + per < nb ? b0 + per : nb;
+  int64_t sum = 0;
+  for (int64_t b = b0; b < b1; ++b) sum += __ldcg(&bin_count[b]);
+  int64_t x = sum;  // inclusive scan over the CTA
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[warp] = x;
+  __syncthreads();
+  int64_t before = 0;
+  for (int w = 0; w < warp; ++w) before += warp_tot[w];
+  int64_t run = before + x - sum;
+  for (int64_t b = b0; b < b1; ++b) {
+    bin_start[b] = run;
+    run += __ldcg(&bin_count[b]);
+  }
+  if (tid == kPrepThreads - 1) bin_start[nb] = before + x;
+}
+
+// Per atom: wrap, Morton key, bin rank, histogram.  With `done`, the last
+// CTA to finish also scans the histogram into bin_start.
+__global__ void __launch_bounds__(kPrepThreads)
+    k_prep(GridParams g, const double* __restrict__ pos, int64_t n,
+           const int32_t* __restrict__ rank_of_bin, uint64_t* __restrict__ key,
+           int32_t* __restrict__ rank, int32_t* __restrict__ bin_count,
+           int64_t* __restrict__ bin_start, int32_t* __restrict__ done) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const AtomWrap w = wrap_atom(g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
-  const int64_t lin = w.bin[0] + (int64_t)g.nb[0] * (w.bin[1] + (int64_t)g.nb[1] * w.bin[2]);
-  const int32_t r = rank_of_bin[lin];
-  key[i] = w.key;
-  rank[i] = r;
-  atomicAdd(&bin_count[r], 1);
+  if (i < n) {
+    const AtomWrap w = wrap_atom(g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+    const int64_t lin = w.bin[0] + (int64_t)g.nb[0] * (w.bin[1] + (int64_t)g.nb[1] * w.bin[2]);
+    const int32_t r = rank_of_bin[lin];
+    key[i] = w.key;
+    rank[i] = r;
+    atomicAdd(&bin_count[r], 1);
+  }
+  if (!done) return;
+  __shared__ int last;
+  __threadfence();  // this CTA's histogram updates before its completion count
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(done, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  cta_bin_scan(bin_count, g.total_bins, bin_start);
 }
 
 __global__ void k_scatter(const uint64_t* __restrict__ key, const int32_t* __restrict__ rank,
@@ -311,9 +356,11 @@ void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const 
     k_rank_table<<<(unsigned)((g.total_bins + T - 1) / T), T, 0, s>>>(g, b.rank_of_bin);
     note_launches(1);
   }
-  k_prep<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(g, pos, n, b.rank_of_bin, b.key, b.rank,
-                                                    b.bin_count);
-  exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
+  const bool fused = b.build_done != nullptr && g.total_bins <= kFusedBinScanMax;
+  k_prep<<<(unsigned)((n + kPrepThreads - 1) / kPrepThreads), kPrepThreads, 0, s>>>(
+      g, pos, n, b.rank_of_bin, b.key, b.rank, b.bin_count, b.bin_start,
+      fused ? b.build_done : nullptr);
+  if (!fused) exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
   k_scatter<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(b.key, b.rank, n, b.bin_start, b.bin_fill,
                                                        b.skey, b.sidx);
   k_binsort<<<(unsigned)g.total_bins, kSortThreads, 0, s>>>(

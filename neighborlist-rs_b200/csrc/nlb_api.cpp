@@ -411,9 +411,10 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
                           c.rank_nb[0] == sp.grid.nb[0] && c.rank_nb[1] == sp.grid.nb[1] &&
                           c.rank_nb[2] == sp.grid.nb[2];
     // One zeroed block: bin histogram, scatter cursors, pair-task counters.
-    int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 2);
+    int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 4);
     b.bin_count = zeroed;
     b.bin_fill = zeroed ? zeroed + nb : nullptr;
+    b.build_done = zeroed ? zeroed + 2 * nb + 2 : nullptr;
     b.bin_start = slot<int64_t>(c, kSlotBinStart, nb + 1);
     b.key = slot<uint64_t>(c, kSlotKey, n);
     b.rank = slot<int32_t>(c, kSlotRank, n);
@@ -445,7 +446,7 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
     if (!b.rank_of_bin || !b.bin_count || !b.bin_fill || !b.bin_start || !b.key || !b.rank ||
         !b.skey || !b.sidx || !b.skey2 || !b.sidx2 || !b.px || !b.py || !b.pz || !b.meta)
       return fail(NLB_ERR_NOMEM, "device allocation failed");
-    cudaMemsetAsync(zeroed, 0, sizeof(int32_t) * (2 * (size_t)nb + 2), s);
+    cudaMemsetAsync(zeroed, 0, sizeof(int32_t) * (2 * (size_t)nb + 4), s);
     launch_grid_build(sp.grid, d_pos, n, b, s, !same_tab);
     for (int a = 0; a < 3; ++a) c.rank_nb[a] = sp.grid.nb[a];
   }

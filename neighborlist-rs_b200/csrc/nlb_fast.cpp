@@ -93,12 +93,13 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   sp.rank_cached = b.rank_of_bin == tab_before && tab_cap > 0 && c.rank_nb[0] == sp.grid.nb[0] &&
                    c.rank_nb[1] == sp.grid.nb[1] && c.rank_nb[2] == sp.grid.nb[2];
   // Zeroed block: bin histogram, scatter cursors, 2 task counters, 64-bit
-  // mask cursor (8-byte aligned: 2 nb + 2 is even).
-  int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 4);
+  // mask cursor (8-byte aligned: 2 nb + 2 is even), build completion count.
+  int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 6);
   b.bin_count = zeroed;
   b.bin_fill = zeroed ? zeroed + nb : nullptr;
   b.counters = zeroed ? zeroed + 2 * nb : nullptr;
   b.mask_top = zeroed ? reinterpret_cast<unsigned long long*>(zeroed + 2 * nb + 2) : nullptr;
+  b.build_done = zeroed ? zeroed + 2 * nb + 4 : nullptr;
   const int64_t max_tasks = (n / 32 + std::min<int64_t>(n, nb) + 1) * cells;
   b.task_hdr = slot<int4>(c, kSlotTaskHdr, max_tasks);
   b.masks = slot<uint32_t>(c, kSlotMasks, mask_cap);
@@ -148,7 +149,7 @@ void issue_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t capacity) {
   const int64_t n = sp.n;
   const int64_t nb = sp.grid.total_bins;
   c.mark(0);
-  cudaMemsetAsync(sp.gb.bin_count, 0, sizeof(int32_t) * (2 * (size_t)nb + 4), s);
+  cudaMemsetAsync(sp.gb.bin_count, 0, sizeof(int32_t) * (2 * (size_t)nb + 6), s);
   launch_grid_build(sp.grid, d_pos, n, sp.gb, s, !sp.rank_cached);
   c.mark(1);
   launch_pair_count(sp.grid, sp.gb, n, sp.band, sp.counts, s);

@@ -51,6 +51,10 @@ struct GridBuffers {
   int32_t* irr_list;
   uint8_t* irr;
   int32_t* counters;
+  // Optional (zeroed by the caller before the build): completion counter of
+  // k_prep, whose last CTA then scans the bin histogram into bin_start
+  // itself (grids of at most kFusedBinScanMax bins); nullptr: separate scan.
+  int32_t* build_done;
   // Optional (masks == nullptr: the emit pass recomputes every test): the
   // count pass stores, per pair task, the candidate range, image shift and a
   // 32-bit hit mask per lane per 32-candidate chunk in `masks` (bump-
@@ -62,6 +66,8 @@ struct GridBuffers {
   unsigned long long* mask_top;
   int64_t mask_cap;
 };
+
+constexpr int64_t kFusedBinScanMax = 65536;
 
 // need_rank_table = false reuses rank_of_bin from a previous build with the
 // same bins per axis.
