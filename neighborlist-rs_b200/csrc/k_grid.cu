@@ -127,6 +127,7 @@ __global__ void k_scatter(const uint64_t* __restrict__ key, const int32_t* __res
                           int64_t n, const int64_t* __restrict__ bin_start,
                           int32_t* __restrict__ bin_fill, uint64_t* __restrict__ skey,
                           int32_t* __restrict__ sidx) {
+  pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int32_t r = rank[i];
@@ -180,6 +181,7 @@ __global__ void __launch_bounds__(kSortThreads)
               uint8_t* __restrict__ irr, int32_t* __restrict__ counters) {
   __shared__ uint64_t sk[kSortCap];
   __shared__ int32_t sv[kSortCap];
+  pdl_wait();
   const int64_t r = blockIdx.x;
   const int64_t s = bin_start[r];
   const int64_t e = bin_start[r + 1];
@@ -361,11 +363,11 @@ void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const 
       g, pos, n, b.rank_of_bin, b.key, b.rank, b.bin_count, b.bin_start,
       fused ? b.build_done : nullptr);
   if (!fused) exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
-  k_scatter<<<(unsigned)((n + T - 1) / T), T, 0, s>>>(b.key, b.rank, n, b.bin_start, b.bin_fill,
-                                                       b.skey, b.sidx);
-  k_binsort<<<(unsigned)g.total_bins, kSortThreads, 0, s>>>(
-      g, pos, b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta, b.p32,
-      b.sbin, b.groups, b.irr_list, b.irr, b.counters);
+  launch_pdl(k_scatter, dim3((unsigned)((n + T - 1) / T)), dim3(T), 0, s, b.key, b.rank, n,
+             b.bin_start, b.bin_fill, b.skey, b.sidx);
+  launch_pdl(k_binsort, dim3((unsigned)g.total_bins), dim3(kSortThreads), 0, s, g, pos,
+             b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta, b.p32,
+             b.sbin, b.groups, b.irr_list, b.irr, b.counters);
   note_launches(3);
 }
 

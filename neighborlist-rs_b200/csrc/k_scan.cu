@@ -48,6 +48,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ int64_t s_prefix;
   __shared__ int s_tile;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  pdl_wait();
   if (tid == 0) s_tile = (int)atomicAdd(reinterpret_cast<unsigned long long*>(&state[0]), 1ull);
   __syncthreads();
   const int tile = s_tile;
@@ -165,10 +166,12 @@ static_assert(sizeof(int64_t) * ((kTile / 2) + (kTile / 2) / 32) <=
               "the output stage must fit in the input stage");
 
 template <class TIn>
-void scan_impl(const TIn* in, int64_t n, int64_t* out, int64_t* tmp, cudaStream_t s) {
+void scan_impl(const TIn* in, int64_t n, int64_t* out, int64_t* tmp, cudaStream_t s,
+               bool zero_state = true) {
   const int64_t tiles = n > 0 ? (n + kTile - 1) / kTile : 1;
-  cudaMemsetAsync(tmp, 0, sizeof(int64_t) * (size_t)(tiles + 2), s);
-  k_scan<TIn><<<(unsigned)tiles, kThreads, 0, s>>>(in, n, out, reinterpret_cast<uint64_t*>(tmp));
+  if (zero_state) cudaMemsetAsync(tmp, 0, sizeof(int64_t) * (size_t)(tiles + 2), s);
+  launch_pdl(k_scan<TIn>, dim3((unsigned)tiles), dim3(kThreads), 0, s, in, n, out,
+             reinterpret_cast<uint64_t*>(tmp));
   note_launches(1);
 }
 
@@ -184,6 +187,11 @@ void exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, int64_t* tm
 void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* tmp,
                         cudaStream_t s) {
   scan_impl<int32_t>(in, n, out, tmp, s);
+}
+
+void exclusive_scan_u32_zeroed(const uint32_t* in, int64_t n, int64_t* out, int64_t* tmp,
+                               cudaStream_t s) {
+  scan_impl<uint32_t>(in, n, out, tmp, s, false);
 }
 
 }  // namespace nlb

@@ -71,18 +71,6 @@ __device__ __forceinline__ CellDesc describe_cell(const GridParams& g, const Gri
   return d;
 }
 
-__device__ __forceinline__ void bin_centre(const GridParams& g, int32_t lin, double c[3]) {
-  const int32_t bx = lin % g.nb[0];
-  const int32_t by = (lin / g.nb[0]) % g.nb[1];
-  const int32_t bz = lin / (g.nb[0] * g.nb[1]);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    double v = dadd(g.origin[k], dmul(g.basis[0][k], (double)bx));
-    v = dadd(v, dmul(g.basis[1][k], (double)by));
-    c[k] = dadd(v, dmul(g.basis[2][k], (double)bz));
-  }
-}
-
 // One warp per irregular atom: every stencil cell of its own home stencil in
 // order, candidates 32 at a time across lanes (FP64, like k_search.cu).
 template <bool EMIT>
@@ -198,6 +186,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : 3)
   float* sz = reinterpret_cast<float*>(stage_z[warp]);
   int32_t* sw = reinterpret_cast<int32_t*>(stage_w[warp]);
   SlotMeta* smt = stage_m[warp];
+  pdl_wait();
   int64_t* dst0 = EMIT ? t.dst[0] : nullptr;
   if (EMIT && t.total_dev) {
     const int64_t m_total = *t.total_dev;
@@ -494,8 +483,9 @@ void launch_pair_count(const GridParams& g, const GridBuffers& b, int64_t n,
                        const GuardBand& band, uint32_t* counts, cudaStream_t s) {
   EmitTargets t{};
   const int32_t cells = stencil_cells(g);
-  k_pair_tasks<false><<<pair_grid((const void*)k_pair_tasks<false>, 0), kPairWarps * 32, 0, s>>>(
-      g, b, n, cells, band, counts, nullptr, t);
+  launch_pdl(k_pair_tasks<false>, dim3(pair_grid((const void*)k_pair_tasks<false>, 0)),
+             dim3(kPairWarps * 32), 0, s, g, b, n, cells, band, counts,
+             (const int64_t*)nullptr, t);
   note_launches(1);
 }
 
@@ -504,8 +494,9 @@ void launch_pair_emit(const GridParams& g, const GridBuffers& b, int64_t n,
                       cudaStream_t s) {
   const int32_t cells = stencil_cells(g);
   ensure_smem_attr((const void*)k_pair_tasks<true>, (int)kEmitSmem);
-  k_pair_tasks<true><<<pair_grid((const void*)k_pair_tasks<true>, kEmitSmem), kPairWarps * 32,
-                       kEmitSmem, s>>>(g, b, n, cells, band, nullptr, offs, t);
+  launch_pdl(k_pair_tasks<true>, dim3(pair_grid((const void*)k_pair_tasks<true>, kEmitSmem)),
+             dim3(kPairWarps * 32), kEmitSmem, s, g, b, n, cells, band, (uint32_t*)nullptr,
+             offs, t);
   note_launches(1);
 }
 

@@ -152,6 +152,29 @@ __device__ __forceinline__ AtomWrap wrap_atom(const GridParams& g, double px, do
   return w;
 }
 
+// Programmatic dependent launch: a kernel launched with launch_pdl may start
+// while its predecessor in the stream drains; pdl_wait() blocks until the
+// predecessor grid has completed and its writes are visible (a no-op when
+// the kernel was launched normally).  Every kernel launched with launch_pdl
+// calls pdl_wait() before it reads anything its predecessors wrote.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 #endif  // __CUDACC__
 
 }  // namespace nlb

@@ -93,8 +93,13 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   sp.rank_cached = b.rank_of_bin == tab_before && tab_cap > 0 && c.rank_nb[0] == sp.grid.nb[0] &&
                    c.rank_nb[1] == sp.grid.nb[1] && c.rank_nb[2] == sp.grid.nb[2];
   // Zeroed block: bin histogram, scatter cursors, 2 task counters, 64-bit
-  // mask cursor (8-byte aligned: 2 nb + 2 is even), build completion count.
-  int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 6);
+  // mask cursor (8-byte aligned: 2 nb + 2 is even), build completion count,
+  // then the offsets scan's state (8-byte aligned at 2 nb + 6), so a single
+  // memset at the start clears everything and the kernels follow each other
+  // directly.
+  sp.zeroed_words = 2 * (size_t)nb + 6 + 2 * (size_t)scan_tmp_elems(row);
+  int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, sp.zeroed_words);
+  sp.scan_state = zeroed ? reinterpret_cast<int64_t*>(zeroed + 2 * nb + 6) : nullptr;
   b.bin_count = zeroed;
   b.bin_fill = zeroed ? zeroed + nb : nullptr;
   b.counters = zeroed ? zeroed + 2 * nb : nullptr;
@@ -149,12 +154,12 @@ void issue_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t capacity) {
   const int64_t n = sp.n;
   const int64_t nb = sp.grid.total_bins;
   c.mark(0);
-  cudaMemsetAsync(sp.gb.bin_count, 0, sizeof(int32_t) * (2 * (size_t)nb + 6), s);
+  cudaMemsetAsync(sp.gb.bin_count, 0, sizeof(int32_t) * sp.zeroed_words, s);
   launch_grid_build(sp.grid, d_pos, n, sp.gb, s, !sp.rank_cached);
   c.mark(1);
   launch_pair_count(sp.grid, sp.gb, n, sp.band, sp.counts, s);
   c.mark(2);
-  exclusive_scan_u32(sp.counts, sp.row, sp.offs, sp.gb.scan_tmp, s);
+  exclusive_scan_u32_zeroed(sp.counts, sp.row, sp.offs, sp.scan_state, s);
   c.mark(3);
   c.mark(4);
   launch_pair_emit(sp.grid, sp.gb, n, sp.band, sp.offs, fast_targets(sp, capacity), s);
@@ -238,7 +243,7 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
   cudaError_t e = cudaMemcpyAsync(c.h_small, sp.offs + sp.row, sizeof(int64_t),
                                   cudaMemcpyDeviceToHost, c.stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(c.h_small + 1, sp.gb.scan_tmp + 1, sizeof(int64_t),
+    e = cudaMemcpyAsync(c.h_small + 1, sp.scan_state + 1, sizeof(int64_t),
                         cudaMemcpyDeviceToHost, c.stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(c.h_small + 2, sp.gb.mask_top, sizeof(int64_t), cudaMemcpyDeviceToHost,

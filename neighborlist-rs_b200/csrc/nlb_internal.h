@@ -129,6 +129,8 @@ struct SystemPlan {
   int64_t* offs = nullptr;
   int64_t row = 0;              // length of one cutoff's count row
   bool rank_cached = false;     // fast path: rank table reusable
+  int64_t* scan_state = nullptr;  // fast path: offsets-scan state (in the zeroed block)
+  size_t zeroed_words = 0;        // fast path: int32 words cleared at the start of a run
   int64_t* out_src = nullptr;   // fast path: [src | dst] arena
   int32_t* out_sh = nullptr;    // fast path: shift arena
   CutoffSet pass(int32_t g0) const;

@@ -17,6 +17,10 @@ void exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, int64_t* tm
                         cudaStream_t s);
 void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* tmp,
                         cudaStream_t s);
+// As exclusive_scan_u32 with a state buffer (scan_tmp_elems(n) words) that
+// the caller has already zeroed in stream order.
+void exclusive_scan_u32_zeroed(const uint32_t* in, int64_t n, int64_t* out, int64_t* tmp,
+                               cudaStream_t s);
 
 // ---- k_grid.cu : cell-list build (src/search.rs:92-264)
 // Buffers for one system's grid; all device pointers.
