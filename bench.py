@@ -692,10 +692,15 @@ def served_measurements(nl):
     plain(full)
     res = {"plain_per_request_loop": plain(full)}
     with Server(hbm_budget_bytes=40 << 30, workers=2, max_batch=4096) as srv:
-        run_stream(srv, full, None)
+        # Each worker grows its workspace (a device-synchronising reallocation)
+        # the first time it meets a larger request, and results of new sizes
+        # take new pinned blocks: warm every path until that has settled.
+        for _ in range(3):
+            run_stream_raw(srv, full, device=True)
+        for _ in range(2):
+            run_stream(srv, full, None)
         res["saturated_python_api"] = run_stream(srv, full, None)
         res["saturated_c_abi"] = run_stream_raw(srv, full)
-        run_stream_raw(srv, full, device=True)
         res["saturated_c_abi_device_results"] = run_stream_raw(srv, full, device=True)
         res["poisson_100"] = run_stream(srv, full, 100, seed=100)
     out["full_range_sample_48"] = dict(
