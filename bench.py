@@ -46,6 +46,9 @@ for _p in (ROOT, PKG_DIR):
 import numpy as np  # noqa: E402
 
 METRIC = "edges/s (exact edges; cluster-liquid N=10008 PBC rc=6)"
+# (cutoff, pass) -> dram__bytes_read.sum + dram__bytes_write.sum per launch.
+NCU_TRAFFIC = {(6.0, "emit"): 4.865e6, (6.0, "count"): 0.454e6,
+               (14.0, "emit"): 154.38e6, (14.0, "count"): 0.446e6}
 UNIT = "edges/s"
 WORKLOAD = "cluster_liquid N=10008 (1112 x 9-atom clusters) cubic L=46.4 A full PBC rc=6.0 A"
 
@@ -401,6 +404,10 @@ def run_b200(args):
     dominant = "emit" if ph["emit"] >= ph["count"] else "count"
     alg = bytes_emit if dominant == "emit" else bytes_count
     achieved = alg / (ph[dominant] * 1e-3) / 1e9
+    # DRAM bytes (read + write) per launch of the same kernel on the same
+    # workload, from the ncu captures summarised in
+    # profiles/k_pair_tasks_cluster_liquid.md (not measured by this run).
+    traffic = NCU_TRAFFIC.get((float(args.rc), dominant))
     kernel_name = {"emit": "k_pair_tasks<1> (emit pass)",
                    "count": "k_pair_tasks<0> (count pass)"}[dominant]
 
@@ -425,7 +432,9 @@ def run_b200(args):
         "clocks": clk.summary(),
         "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "algorithmic_bytes": alg, "kernel_ms": ph[dominant], "traffic": None,
+                     "algorithmic_bytes": alg, "kernel_ms": ph[dominant], "traffic": traffic,
+                     "traffic_source": "ncu capture (profiles/k_pair_tasks_cluster_liquid.md)"
+                     if traffic is not None else None,
                      "phases_ms": ph},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n + 72,
                 "d2h_bytes_per_step": 28 * m_e2e},
