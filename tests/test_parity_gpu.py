@@ -354,3 +354,52 @@ def test_dense_system_emit_paths(nl, oracle, rc):
     got = nl.build_neighborlists(nl.PyCell(h.tolist()), pos, rc)
     ref = oracle.search_single(pos, h, PBC3, rc, nthreads=16)
     assert_same(got, ref, f"dense liquid rc {rc}")
+
+
+@pytest.mark.parametrize("cell", [True, False])
+def test_non_finite_positions(nl, oracle, cell):
+    """NaN and infinite coordinates follow the reference's saturating casts
+    (NaN -> 0) and NaN-ignoring auto-box bounds: same edges as the oracle."""
+    rng = np.random.default_rng(23)
+    pos = rng.random((1500, 3)) * 25.0
+    pos[7] = [np.nan, 3.0, 4.0]
+    pos[100] = [np.inf, 1.0, 2.0]
+    pos[200, 2] = -np.inf
+    pos[300] = [np.nan, np.nan, np.nan]
+    h = np.eye(3) * 25.0 if cell else None
+    got = nl.build_neighborlists(nl.PyCell(h.tolist()) if cell else None, pos, 5.0)
+    ref = oracle.search_single(pos, h, PBC3 if cell else None, 5.0, nthreads=8)
+    assert_same(got, ref, f"non-finite positions (cell={cell})")
+
+
+def test_concurrent_host_threads(nl):
+    """Builds from several host threads at once (each thread has its own
+    stream and workspace) give the single-threaded results."""
+    import threading
+
+    from neighborlist_rs import workloads as W
+
+    systems = [W.cluster_liquid(n_clusters=150 + 40 * k, box=24.0 + 2 * k, seed=k)
+               for k in range(6)]
+    cells = [nl.PyCell(r.T.tolist()) for _, r in systems]
+    expected = [nl.build_neighborlists(c, p, 6.0) for c, (p, _) in zip(cells, systems)]
+    got = {}
+    errors = []
+
+    def worker(t):
+        try:
+            for rep in range(5):
+                for k in range(len(systems)):
+                    i = (k + t) % len(systems)
+                    got[(t, rep, i)] = nl.build_neighborlists(cells[i], systems[i][0], 6.0)
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(4)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors
+    for (t, rep, i), r in got.items():
+        assert_same(r, (expected[i]["edge_index"], expected[i]["shift"]), f"thread {t} rep {rep}")
