@@ -311,6 +311,8 @@ void release_thread_ctx() {
     cudaStreamSynchronize(c->own_stream);
     for (Ctx::Buf& b : c->bufs)
       if (b.p) cudaFree(b.p);
+    for (Ctx::Buf& b : c->batch_out)
+      if (b.p) cudaFree(b.p);
     for (cudaEvent_t ev : c->ev)
       if (ev) cudaEventDestroy(ev);
     if (c->h_small) cudaFreeHost(c->h_small);

@@ -24,41 +24,43 @@ extern std::atomic<uint64_t> g_bf_threshold;
 
 namespace {
 
-// Grow-only device array that keeps its contents when it grows.
-struct GrowBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  bool reserve(size_t need, cudaStream_t s) {
-    if (need <= bytes) return true;
-    size_t cap = std::max<size_t>(need + need / 2, 1 << 16);
-    void* q = nullptr;
-    if (cudaMalloc(&q, cap) != cudaSuccess) {
-      cudaGetLastError();
-      return false;
-    }
-    if (p) {
-      cudaMemcpyAsync(q, p, bytes, cudaMemcpyDeviceToDevice, s);
-      cudaStreamSynchronize(s);
-      cudaFree(p);
-    }
-    p = q;
-    bytes = cap;
-    return true;
+// Grows a context buffer to `need` bytes, keeping its first `used` bytes
+// (a device-to-device copy and a free of the old block, only on growth).
+bool grow_keep(Ctx::Buf& b, size_t need, size_t used, cudaStream_t s) {
+  if (need <= b.cap) return true;
+  const size_t cap = std::max<size_t>(need + need / 2, 1 << 16);
+  void* q = nullptr;
+  if (cudaMalloc(&q, cap) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
   }
-  ~GrowBuf() {
-    if (p) cudaFree(p);
+  if (b.p) {
+    if (used) cudaMemcpyAsync(q, b.p, used, cudaMemcpyDeviceToDevice, s);
+    cudaStreamSynchronize(s);
+    cudaFree(b.p);
   }
-};
+  b.p = q;
+  b.cap = cap;
+  return true;
+}
 
+// The k output lists of one batched call, in the context's persistent
+// buffers (allocation only when a call needs more than any before it).
 struct Outputs {
-  std::vector<GrowBuf> src, dst, shf;
+  Ctx& c;
   std::vector<int64_t> total;
-  explicit Outputs(int32_t k) : src(k), dst(k), shf(k), total(k, 0) {}
+  Outputs(Ctx& ctx, int32_t k) : c(ctx), total(k, 0) {
+    if (c.batch_out.size() < 3 * (size_t)k) c.batch_out.resize(3 * (size_t)k);
+  }
+  void* src(int32_t q) const { return c.batch_out[3 * q].p; }
+  void* dst(int32_t q) const { return c.batch_out[3 * q + 1].p; }
+  void* shf(int32_t q) const { return c.batch_out[3 * q + 2].p; }
   bool reserve(const std::vector<int64_t>& add, cudaStream_t s) {
     for (size_t q = 0; q < total.size(); ++q) {
-      const size_t need = (size_t)(total[q] + add[q]);
-      if (!src[q].reserve(8 * need, s) || !dst[q].reserve(8 * need, s) ||
-          !shf[q].reserve(12 * need, s))
+      const size_t used = (size_t)total[q], need = (size_t)(total[q] + add[q]);
+      if (!grow_keep(c.batch_out[3 * q], 8 * need, 8 * used, s) ||
+          !grow_keep(c.batch_out[3 * q + 1], 8 * need, 8 * used, s) ||
+          !grow_keep(c.batch_out[3 * q + 2], 12 * need, 12 * used, s))
         return false;
     }
     return true;
@@ -151,9 +153,9 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
     EmitTargets t;
     std::memset(&t, 0, sizeof(t));
     for (int32_t q = 0; q < cs.k; ++q) {
-      t.src[q] = static_cast<int64_t*>(out.src[g0 + q].p);
-      t.dst[q] = static_cast<int64_t*>(out.dst[g0 + q].p);
-      t.sh[q] = static_cast<int32_t*>(out.shf[g0 + q].p);
+      t.src[q] = static_cast<int64_t*>(out.src(g0 + q));
+      t.dst[q] = static_cast<int64_t*>(out.dst(g0 + q));
+      t.sh[q] = static_cast<int32_t*>(out.shf(g0 + q));
       t.base[q] = out.total[g0 + q];
     }
     cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
@@ -230,7 +232,7 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
       cudaMemsetAsync(d_has, 1, (size_t)n_sys, s);
   }
 
-  Outputs out(k);
+  Outputs out(*c, k);
   int32_t i = 0;
   while (i < n_sys) {
     const int64_t ni = starts[i + 1] - starts[i];
@@ -261,9 +263,9 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
     L.dst.resize(k);
     L.sh.resize(k);
     for (int32_t q = 0; q < k; ++q) {
-      L.src[q] = static_cast<int64_t*>(out.src[q].p);
-      L.dst[q] = static_cast<int64_t*>(out.dst[q].p);
-      L.sh[q] = static_cast<int32_t*>(out.shf[q].p);
+      L.src[q] = static_cast<int64_t*>(out.src(q));
+      L.dst[q] = static_cast<int64_t*>(out.dst(q));
+      L.sh[q] = static_cast<int32_t*>(out.shf(q));
     }
     st = emit_system(*c, sp, d_pos + 3 * starts[i], L, out.total.data(), starts[i]);
     if (!st.ok()) return st;
@@ -277,9 +279,9 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
     if (!st.ok()) return st;
     const int64_t m = out.total[q];
     if (m == 0) continue;
-    cudaMemcpyAsync(r.edge_index, out.src[q].p, 8 * m, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(r.edge_index + m, out.dst[q].p, 8 * m, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(r.shift, out.shf[q].p, 12 * m, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(r.edge_index, out.src(q), 8 * m, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(r.edge_index + m, out.dst(q), 8 * m, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(r.shift, out.shf(q), 12 * m, cudaMemcpyDeviceToHost, s);
   }
   cudaError_t e = cudaStreamSynchronize(s);
   if (c->prof) c->harvest();

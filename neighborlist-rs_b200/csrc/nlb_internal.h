@@ -68,6 +68,9 @@ struct Ctx {
   cudaStream_t stream = nullptr;  // active stream: the caller's (nlb_set_stream) or own_stream
   int64_t* h_small = nullptr;     // pinned scratch for small device->host reads
   Buf bufs[kSlotCount];
+  // Batched outputs: [src, dst, shift] per cutoff, grow-only and kept across
+  // calls (results are appended run by run, so growth preserves contents).
+  std::vector<Buf> batch_out;
   // Phase timing (nlb_profile): events ev[0..3] bracket build / count / scan,
   // ev[4..5] the emit pass; harvested after the stream is synchronized.
   bool prof = false;
