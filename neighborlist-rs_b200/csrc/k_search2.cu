@@ -1,5 +1,6 @@
-// k_search2.cu -- single-cutoff stencil search as (atom group, stencil cell)
-// pair tasks, with an FP32 pair test and an exact FP64 guard-band recheck.
+// k_search2.cu -- stencil search for one to four cutoffs as (atom group,
+// stencil cell) pair tasks, with an FP32 pair test and an exact FP64
+// guard-band recheck.
 //
 // Same edges, same order as k_search.cu and the reference.  The canonical
 // order is (sorted atom, stencil cell in x/y/z order, candidate in bin
@@ -18,11 +19,19 @@
 //   d2_32 >= rc^2 + delta a certain miss; in between, the reference's exact
 //   FP64 expression (x_j - x_i) + off on the FP64 wrapped positions decides
 //   (src/search.rs:540-553).  Results are identical to the FP64 kernels.
+// * Several cutoffs share one traversal of the grid built at the largest
+//   (CellList::par_search_multi, src/search.rs:344-435, 729-893): each
+//   pair's FP32 distance is compared with every cutoff's band and an
+//   ambiguous pair is rechecked once in FP64 against all of them; list q
+//   then has its edges in the same canonical order.  Disjoint shells give a
+//   pair to the first cutoff it falls inside (src/search.rs:845-848), so
+//   list q drops the pairs inside cutoff q - 1.
 // * Atoms whose home stencil differs from their stored bin (the search
 //   recomputes the home bin from the wrapped position, src/search.rs:454-457;
 //   this differs only within rounding of a bin face) are skipped by the
 //   tasks and handled by one warp each, in FP64, with the same outputs.
 #include <cmath>
+#include <cstring>
 
 #include "k_traverse.cuh"
 
@@ -72,15 +81,18 @@ __device__ __forceinline__ CellDesc describe_cell(const GridParams& g, const Gri
 }
 
 // One warp per irregular atom: every stencil cell of its own home stencil in
-// order, candidates 32 at a time across lanes (FP64, like k_search.cu).
-template <bool EMIT>
+// order, candidates 32 at a time across lanes (FP64, like k_search.cu), each
+// candidate tested against the K cutoffs.
+template <bool EMIT, int K>
 __device__ void pair_irregular(const GridParams& g, const GridBuffers& b, int32_t n_cells,
-                               double rc_sq, uint32_t* __restrict__ counts,
+                               const PairBands& pb, uint32_t* __restrict__ counts,
                                const int64_t* __restrict__ offs, const EmitTargets& t,
                                int64_t* __restrict__ dst0, int64_t gwarp, int64_t nwarps) {
   const int lane = threadIdx.x & 31;
   const int32_t n_irr = b.counters[1];
-  const int64_t off0 = EMIT ? offs[0] : 0;
+  int64_t off0[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) off0[q] = EMIT ? offs[q * pb.row] : 0;
   for (int64_t w = gwarp; w < n_irr; w += nwarps) {
     const int32_t p = b.irr_list[w];
     const double xi = b.px[p], yi = b.py[p], zi = b.pz[p];
@@ -97,12 +109,18 @@ __device__ void pair_irregular(const GridParams& g, const GridBuffers& b, int32_
       const CellDesc d = describe_cell(g, b, home, c);
       const bool live = !(norm2(dsub(d.cs[0], xi), dsub(d.cs[1], yi), dsub(d.cs[2], zi)) > g.prune_sq);
       const bool shifted = (d.sh[0] | d.sh[1] | d.sh[2]) != 0;
-      uint32_t cnt = 0;
-      int64_t slot = EMIT ? t.base[0] + (offs[(int64_t)p * n_cells + c] - off0) : 0;
+      uint32_t cnt[K];
+      int64_t slot[K];
+#pragma unroll
+      for (int q = 0; q < K; ++q) {
+        cnt[q] = 0;
+        slot[q] = EMIT ? t.base[q] + (offs[q * pb.row + (int64_t)p * n_cells + c] - off0[q]) : 0;
+      }
       if (live) {
         for (int32_t jb = d.b0; jb < d.b1; jb += 32) {
           const int32_t j = jb + lane;
-          bool hit = false;
+          bool ord = false;
+          double d2 = 0.0;
           int32_t jo = 0;
           SlotMeta mj{};
           if (j < d.b1) {
@@ -111,26 +129,35 @@ __device__ void pair_irregular(const GridParams& g, const GridBuffers& b, int32_
             const double ez = dadd(dsub(b.pz[j], zi), d.off[2]);
             mj = b.meta[j];
             jo = mj.orig;
-            hit = norm2(ex, ey, ez) < rc_sq && (mi.orig < jo || (mi.orig == jo && shifted));
+            d2 = norm2(ex, ey, ez);
+            ord = mi.orig < jo || (mi.orig == jo && shifted);
           }
-          const unsigned m = __ballot_sync(0xffffffffu, hit);
-          if (!EMIT) {
-            cnt += __popc(m);
-          } else {
-            if (hit) {
-              const int64_t e = slot + __popc(m & lanemask_lt());
-              t.src[0][e] = (int64_t)mi.orig + t.index_offset;
-              dst0[e] = (int64_t)jo + t.index_offset;
-              int32_t* sp = t.sh[0] + 3 * e;
-              sp[0] = (mj.sx - mi.sx) + d.sh[0];
-              sp[1] = (mj.sy - mi.sy) + d.sh[1];
-              sp[2] = (mj.sz - mi.sz) + d.sh[2];
+#pragma unroll
+          for (int q = 0; q < K; ++q) {
+            const bool hit = ord && d2 < pb.q[q].rc_sq &&
+                             !(q > 0 && pb.disjoint && d2 < pb.q[q > 0 ? q - 1 : 0].rc_sq);
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (!EMIT) {
+              cnt[q] += __popc(m);
+            } else {
+              if (hit) {
+                const int64_t e = slot[q] + __popc(m & lanemask_lt());
+                t.src[q][e] = (int64_t)mi.orig + t.index_offset;
+                (q == 0 ? dst0 : t.dst[q])[e] = (int64_t)jo + t.index_offset;
+                int32_t* sp = t.sh[q] + 3 * e;
+                sp[0] = (mj.sx - mi.sx) + d.sh[0];
+                sp[1] = (mj.sy - mi.sy) + d.sh[1];
+                sp[2] = (mj.sz - mi.sz) + d.sh[2];
+              }
+              slot[q] += __popc(m);
             }
-            slot += __popc(m);
           }
         }
       }
-      if (!EMIT && lane == 0) counts[(int64_t)p * n_cells + c] = cnt;
+      if (!EMIT && lane == 0) {
+#pragma unroll
+        for (int q = 0; q < K; ++q) counts[q * pb.row + (int64_t)p * n_cells + c] = cnt[q];
+      }
     }
   }
 }
@@ -151,12 +178,13 @@ __device__ __forceinline__ void div_mod_fast(int32_t v, int32_t m, int32_t& rem,
   }
 }
 
-// Register budgets measured best on B200: the count pass at 3 CTAs per SM;
-// the emit pass unbounded (120 registers, 2 CTAs per SM), which beats a
-// spilling 80-register build.
-template <bool EMIT>
-__global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : 3)
-    k_pair_tasks(GridParams g, GridBuffers b, int64_t n, int32_t n_cells, GuardBand band,
+// Register budgets measured best on B200: the single-cutoff count pass at 3
+// CTAs per SM (2 with several cutoffs, which need more masks live); the emit
+// pass unbounded (120 registers, 2 CTAs per SM), which beats a spilling
+// 80-register build.
+template <bool EMIT, int K>
+__global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
+    k_pair_tasks(GridParams g, GridBuffers b, int64_t n, int32_t n_cells, PairBands pb,
                  uint32_t* __restrict__ counts, const int64_t* __restrict__ offs, EmitTargets t) {
   // Staged candidates as pairs (2m, 2m + 1): {x, x', y, y'}, {z, z'}, {idx, idx'}.
   __shared__ float4 stage_xy[kPairWarps][16];
@@ -195,8 +223,14 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : 3)
   }
   const uint32_t n_tasks = (uint32_t)b.counters[0] * (uint32_t)n_cells;
   const uint32_t step = gridDim.x * kPairWarps;
-  const int64_t off0 = EMIT ? offs[0] : 0;
-  const float lo = band.lo, hi = band.hi;
+  int64_t off0[K];
+  float lo[K], hi[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    off0[q] = EMIT ? offs[q * pb.row] : 0;
+    lo[q] = pb.q[q].lo;
+    hi[q] = pb.q[q].hi;
+  }
 
   for (uint32_t task = blockIdx.x * kPairWarps + warp; task < n_tasks; task += step) {
     const uint32_t gi = task / (uint32_t)n_cells;
@@ -211,95 +245,104 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : 3)
       if (hdr.x == -2) continue;
       if (hdr.x >= 0) {
         const int32_t h0 = hdr.y, h1 = hdr.z;
+        const int32_t words = ((h1 - h0 + 31) >> 5) * 32;  // one cutoff's masks
         const uint32_t pw = (uint32_t)hdr.w;  // three signed 10-bit shifts
         const int32_t s0 = (int32_t)(pw << 22) >> 22;
         const int32_t s1 = (int32_t)(pw << 12) >> 22;
         const int32_t s2 = (int32_t)(pw << 2) >> 22;
-        int64_t slot = 0;
-        int32_t cnt = 0;
         SlotMeta mi{};
-        if (mine) {
-          const int64_t idx = (int64_t)p * n_cells + c;
-          const int64_t o0 = offs[idx];
-          slot = t.base[0] + (o0 - off0);
-          cnt = (int32_t)(offs[idx + 1] - o0);
-          mi = b.meta[p];
-        }
-        // Stage the task's hits (lane's hits at [pre, pre + cnt)), then write
-        // them with the whole warp in stage order: each lane's (atom, cell)
-        // run is contiguous in the output, so consecutive threads store to
-        // consecutive slots instead of 32 lanes storing to 32 runs.
-        int32_t pre = cnt;
+        if (mine) mi = b.meta[p];
+#pragma unroll 1
+        for (int q = 0; q < K; ++q) {
+          int64_t* __restrict__ srcq = t.src[q];
+          int64_t* __restrict__ dstq = q == 0 ? dst0 : t.dst[q];
+          int32_t* __restrict__ shq = t.sh[q];
+          const uint32_t* mq = b.masks + (int64_t)hdr.x + (int64_t)q * words;
+          int64_t slot = 0;
+          int32_t cnt = 0;
+          if (mine) {
+            const int64_t idx = q * pb.row + (int64_t)p * n_cells + c;
+            const int64_t o0 = offs[idx];
+            slot = t.base[q] + (o0 - off0[q]);
+            cnt = (int32_t)(offs[idx + 1] - o0);
+          }
+          // Stage the task's hits (lane's hits at [pre, pre + cnt)), then
+          // write them with the whole warp in stage order: each lane's
+          // (atom, cell) run is contiguous in the output, so consecutive
+          // threads store to consecutive slots instead of 32 lanes storing to
+          // 32 runs.
+          int32_t pre = cnt;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int32_t y = __shfl_up_sync(0xffffffffu, pre, o);
-          if (lane >= o) pre += y;
-        }
-        const int32_t total = __shfl_sync(0xffffffffu, pre, 31);
-        pre -= cnt;
-        if (total <= kStageCap && h1 - h0 <= 65536) {
-          uint32_t* st = stage_hits + warp * kStageCap;
-          lane_base[warp][lane] = slot - pre;
-          lane_meta[warp][lane] = mi;
-          int32_t r = pre;
-          const int32_t r_end = pre + cnt;  // the lane's own stage range
-          for (int32_t jb = h0; jb < h1; jb += 32) {
-            uint32_t hits = mine ? b.masks[(int64_t)hdr.x + (jb - h0) + lane] : 0u;
-            while (hits) {
-              const int jj = __ffs(hits) - 1;
-              hits &= hits - 1;
-              if (r < r_end) st[r] = ((uint32_t)lane << 16) | (uint32_t)(jb - h0 + jj);
-              ++r;
+          for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += y;
+          }
+          const int32_t total = __shfl_sync(0xffffffffu, pre, 31);
+          pre -= cnt;
+          if (total <= kStageCap && h1 - h0 <= 65536) {
+            uint32_t* st = stage_hits + warp * kStageCap;
+            lane_base[warp][lane] = slot - pre;
+            lane_meta[warp][lane] = mi;
+            int32_t r = pre;
+            const int32_t r_end = pre + cnt;  // the lane's own stage range
+            for (int32_t jb = h0; jb < h1; jb += 32) {
+              uint32_t hits = mine ? mq[(jb - h0) + lane] : 0u;
+              while (hits) {
+                const int jj = __ffs(hits) - 1;
+                hits &= hits - 1;
+                if (r < r_end) st[r] = ((uint32_t)lane << 16) | (uint32_t)(jb - h0 + jj);
+                ++r;
+              }
+            }
+            __syncwarp();
+            // Four waves at a time: their candidate gathers are in flight
+            // together before any of their stores.
+            for (int32_t k0 = lane; k0 < total; k0 += 4 * 32) {
+              uint32_t v[4];
+              SlotMeta mj[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const int32_t k = k0 + 32 * u;
+                v[u] = k < total ? st[k] : 0u;
+                if (k < total) mj[u] = b.meta[h0 + (int32_t)(v[u] & 0xffffu)];
+              }
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                const int32_t k = k0 + 32 * u;
+                if (k >= total) break;
+                const int l = (int)(v[u] >> 16);
+                const SlotMeta ml = lane_meta[warp][l];
+                const int64_t e = lane_base[warp][l] + k;
+                srcq[e] = (int64_t)ml.orig + t.index_offset;
+                dstq[e] = (int64_t)mj[u].orig + t.index_offset;
+                int32_t* sp = shq + 3 * e;
+                sp[0] = (mj[u].sx - ml.sx) + s0;
+                sp[1] = (mj[u].sy - ml.sy) + s1;
+                sp[2] = (mj[u].sz - ml.sz) + s2;
+              }
+            }
+            __syncwarp();
+          } else {
+            for (int32_t jb = h0; jb < h1; jb += 32) {
+              uint32_t hits = mine ? mq[(jb - h0) + lane] : 0u;
+              if (!__any_sync(0xffffffffu, hits != 0)) continue;
+              if (jb + lane < h1) smt[lane] = b.meta[jb + lane];
+              __syncwarp();
+              while (hits) {
+                const int jj = __ffs(hits) - 1;
+                hits &= hits - 1;
+                const SlotMeta mj = smt[jj];
+                srcq[slot] = (int64_t)mi.orig + t.index_offset;
+                dstq[slot] = (int64_t)mj.orig + t.index_offset;
+                int32_t* sp = shq + 3 * slot;
+                sp[0] = (mj.sx - mi.sx) + s0;
+                sp[1] = (mj.sy - mi.sy) + s1;
+                sp[2] = (mj.sz - mi.sz) + s2;
+                ++slot;
+              }
+              __syncwarp();
             }
           }
-          __syncwarp();
-          // Four waves at a time: their candidate gathers are in flight
-          // together before any of their stores.
-          for (int32_t k0 = lane; k0 < total; k0 += 4 * 32) {
-            uint32_t v[4];
-            SlotMeta mj[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int32_t k = k0 + 32 * u;
-              v[u] = k < total ? st[k] : 0u;
-              if (k < total) mj[u] = b.meta[h0 + (int32_t)(v[u] & 0xffffu)];
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int32_t k = k0 + 32 * u;
-              if (k >= total) break;
-              const int l = (int)(v[u] >> 16);
-              const SlotMeta ml = lane_meta[warp][l];
-              const int64_t e = lane_base[warp][l] + k;
-              t.src[0][e] = (int64_t)ml.orig + t.index_offset;
-              dst0[e] = (int64_t)mj[u].orig + t.index_offset;
-              int32_t* sp = t.sh[0] + 3 * e;
-              sp[0] = (mj[u].sx - ml.sx) + s0;
-              sp[1] = (mj[u].sy - ml.sy) + s1;
-              sp[2] = (mj[u].sz - ml.sz) + s2;
-            }
-          }
-          __syncwarp();
-          continue;
-        }
-        for (int32_t jb = h0; jb < h1; jb += 32) {
-          uint32_t hits = mine ? b.masks[(int64_t)hdr.x + (jb - h0) + lane] : 0u;
-          if (!__any_sync(0xffffffffu, hits != 0)) continue;
-          if (jb + lane < h1) smt[lane] = b.meta[jb + lane];
-          __syncwarp();
-          while (hits) {
-            const int jj = __ffs(hits) - 1;
-            hits &= hits - 1;
-            const SlotMeta mj = smt[jj];
-            t.src[0][slot] = (int64_t)mi.orig + t.index_offset;
-            dst0[slot] = (int64_t)mj.orig + t.index_offset;
-            int32_t* sp = t.sh[0] + 3 * slot;
-            sp[0] = (mj.sx - mi.sx) + s0;
-            sp[1] = (mj.sy - mi.sy) + s1;
-            sp[2] = (mj.sz - mi.sz) + s2;
-            ++slot;
-          }
-          __syncwarp();
         }
         continue;
       }
@@ -332,19 +375,25 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : 3)
     const double xi = b.px[p], yi = b.py[p], zi = b.pz[p];
     const bool live =
         mine && !(norm2(dsub(cs[0], xi), dsub(cs[1], yi), dsub(cs[2], zi)) > g.prune_sq);
-    uint32_t cnt = 0;
-    int64_t slot = 0;
-    if (EMIT && mine) slot = t.base[0] + (offs[(int64_t)p * n_cells + c] - off0);
+    uint32_t cnt[K];
+    int64_t slot[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+      cnt[q] = 0;
+      slot[q] = 0;
+      if (EMIT && mine) slot[q] = t.base[q] + (offs[q * pb.row + (int64_t)p * n_cells + c] - off0[q]);
+    }
     const bool work = __any_sync(0xffffffffu, live) && b1 > b0;
-    // Count pass: reserve this task's hit masks (one word per lane per chunk).
+    const int32_t words = ((b1 - b0 + 31) >> 5) * 32;  // one cutoff's masks
+    // Count pass: reserve this task's hit masks (one word per lane per chunk
+    // per cutoff).
     int32_t mbase = -2;
     if (!EMIT && b.masks) {
       if (work) {
-        const int32_t words = ((b1 - b0 + 31) >> 5) * 32;
         long long top = 0;
-        if (lane == 0) top = (long long)atomicAdd(b.mask_top, (unsigned long long)words);
+        if (lane == 0) top = (long long)atomicAdd(b.mask_top, (unsigned long long)(K * words));
         top = __shfl_sync(0xffffffffu, top, 0);
-        const bool fits = top + words <= b.mask_cap && top + words < 0x7fffffffLL &&
+        const bool fits = top + K * words <= b.mask_cap && top + K * words < 0x7fffffffLL &&
                           sh[0] >= -511 && sh[0] <= 511 && sh[1] >= -511 && sh[1] <= 511 &&
                           sh[2] >= -511 && sh[2] <= 511;
         mbase = fits ? (int32_t)top : -1;
@@ -383,8 +432,11 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : 3)
         __syncwarp();
         // FP32 test of all 32 staged candidates into bit masks, two at a time
         // with the packed FP32 units (element-wise the same roundings as the
-        // scalar dx = x_j + u, d2 = fma(dz, dz, fma(dy, dy, dx * dx))).
-        uint32_t inside = 0, maybe = 0, order = 0;
+        // scalar dx = x_j + u, d2 = fma(dz, dz, fma(dy, dy, dx * dx))), one
+        // squared distance per pair against every cutoff's band.
+        uint32_t inside[K], maybe[K], order = 0;
+#pragma unroll
+        for (int q = 0; q < K; ++q) inside[q] = maybe[q] = 0;
 #pragma unroll
         for (int pr = 0; pr < 16; ++pr) {
           const float4 xy = stage_xy[warp][pr];
@@ -394,13 +446,20 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : 3)
           const float2 dy = __fadd2_rn(make_float2(xy.z, xy.w), uy2);
           const float2 dz = __fadd2_rn(z, uz2);
           const float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-          inside |= ((uint32_t)(d2.x < lo) | ((uint32_t)(d2.y < lo) << 1)) << (2 * pr);
-          maybe |= ((uint32_t)(d2.x < hi) | ((uint32_t)(d2.y < hi) << 1)) << (2 * pr);
+#pragma unroll
+          for (int q = 0; q < K; ++q) {
+            inside[q] |= ((uint32_t)(d2.x < lo[q]) | ((uint32_t)(d2.y < lo[q]) << 1)) << (2 * pr);
+            maybe[q] |= ((uint32_t)(d2.x < hi[q]) | ((uint32_t)(d2.y < hi[q]) << 1)) << (2 * pr);
+          }
           order |= ((uint32_t)(w.x > io_adj) | ((uint32_t)(w.y > io_adj) << 1)) << (2 * pr);
         }
         if (!live) order = 0;
-        // Guard band: the reference's exact FP64 test decides.
-        uint32_t amb = maybe & ~inside & order;
+        // Guard bands: the reference's exact FP64 test decides (for every
+        // cutoff at once; it agrees with the certain FP32 outcomes).
+        uint32_t amb = 0;
+#pragma unroll
+        for (int q = 0; q < K; ++q) amb |= maybe[q] & ~inside[q];
+        amb &= order;
         while (amb) {
           const int jj = __ffs(amb) - 1;
           amb &= amb - 1;
@@ -408,35 +467,55 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : 3)
           const double ex = dadd(dsub(b.px[j], xi), off[0]);
           const double ey = dadd(dsub(b.py[j], yi), off[1]);
           const double ez = dadd(dsub(b.pz[j], zi), off[2]);
-          if (norm2(ex, ey, ez) < band.rc_sq) inside |= 1u << jj;
+          const double d2e = norm2(ex, ey, ez);
+#pragma unroll
+          for (int q = 0; q < K; ++q)
+            if (d2e < pb.q[q].rc_sq) inside[q] |= 1u << jj;
         }
-        uint32_t hits = inside & order;
+        uint32_t hits[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) hits[q] = inside[q] & order;
+        // Disjoint shells: cutoff q keeps only the pairs outside cutoff q - 1.
+        if (K > 1 && pb.disjoint) {
+#pragma unroll
+          for (int q = K - 1; q > 0; --q) hits[q] &= ~inside[q - 1];
+        }
         if (!EMIT) {
-          cnt += __popc(hits);
-          if (mbase >= 0) b.masks[(int64_t)mbase + (jb - b0) + lane] = hits;
+#pragma unroll
+          for (int q = 0; q < K; ++q) {
+            cnt[q] += __popc(hits[q]);
+            if (mbase >= 0) b.masks[(int64_t)mbase + (int64_t)q * words + (jb - b0) + lane] = hits[q];
+          }
         } else {
-          while (hits) {
-            const int jj = __ffs(hits) - 1;
-            hits &= hits - 1;
-            const SlotMeta mj = smt[jj];
-            t.src[0][slot] = (int64_t)io + t.index_offset;
-            dst0[slot] = (int64_t)mj.orig + t.index_offset;
-            int32_t* sp = t.sh[0] + 3 * slot;
-            sp[0] = (mj.sx - mi.sx) + sh[0];
-            sp[1] = (mj.sy - mi.sy) + sh[1];
-            sp[2] = (mj.sz - mi.sz) + sh[2];
-            ++slot;
+#pragma unroll
+          for (int q = 0; q < K; ++q) {
+            int64_t* __restrict__ dstq = q == 0 ? dst0 : t.dst[q];
+            while (hits[q]) {
+              const int jj = __ffs(hits[q]) - 1;
+              hits[q] &= hits[q] - 1;
+              const SlotMeta mj = smt[jj];
+              t.src[q][slot[q]] = (int64_t)io + t.index_offset;
+              dstq[slot[q]] = (int64_t)mj.orig + t.index_offset;
+              int32_t* sp = t.sh[q] + 3 * slot[q];
+              sp[0] = (mj.sx - mi.sx) + sh[0];
+              sp[1] = (mj.sy - mi.sy) + sh[1];
+              sp[2] = (mj.sz - mi.sz) + sh[2];
+              ++slot[q];
+            }
           }
         }
         __syncwarp();
       }
     }
-    if (!EMIT && mine) counts[(int64_t)p * n_cells + c] = cnt;
+    if (!EMIT && mine) {
+#pragma unroll
+      for (int q = 0; q < K; ++q) counts[q * pb.row + (int64_t)p * n_cells + c] = cnt[q];
+    }
   }
   // Atoms whose home stencil is not their stored bin (normally none).
-  pair_irregular<EMIT>(g, b, n_cells, band.rc_sq, counts, offs, t, dst0,
-                       (int64_t)blockIdx.x * kPairWarps + warp, step);
-  if (!EMIT && blockIdx.x == 0 && threadIdx.x == 0) counts[n * (int64_t)n_cells] = 0;
+  pair_irregular<EMIT, K>(g, b, n_cells, pb, counts, offs, t, dst0,
+                          (int64_t)blockIdx.x * kPairWarps + warp, step);
+  if (!EMIT && blockIdx.x == 0 && threadIdx.x < K) counts[threadIdx.x * pb.row + n * (int64_t)n_cells] = 0;
 }
 
 int pair_grid(const void* func, size_t smem) {
@@ -479,25 +558,70 @@ bool make_guard_band(const GridParams& g, double rc, GuardBand& band) {
   return true;
 }
 
-void launch_pair_count(const GridParams& g, const GridBuffers& b, int64_t n,
-                       const GuardBand& band, uint32_t* counts, cudaStream_t s) {
+namespace {
+
+PairBands single_band(const GuardBand& band) {
+  PairBands pb;
+  std::memset(&pb, 0, sizeof(pb));
+  pb.q[0] = band;
+  pb.k = 1;
+  return pb;
+}
+
+template <int K>
+void pair_count_k(const GridParams& g, const GridBuffers& b, int64_t n, const PairBands& pb,
+                  uint32_t* counts, cudaStream_t s) {
   EmitTargets t{};
   const int32_t cells = stencil_cells(g);
-  launch_pdl(k_pair_tasks<false>, dim3(pair_grid((const void*)k_pair_tasks<false>, 0)),
-             dim3(kPairWarps * 32), 0, s, g, b, n, cells, band, counts,
-             (const int64_t*)nullptr, t);
+  launch_pdl(k_pair_tasks<false, K>, dim3(pair_grid((const void*)k_pair_tasks<false, K>, 0)),
+             dim3(kPairWarps * 32), 0, s, g, b, n, cells, pb, counts, (const int64_t*)nullptr, t);
   note_launches(1);
+}
+
+template <int K>
+void pair_emit_k(const GridParams& g, const GridBuffers& b, int64_t n, const PairBands& pb,
+                 const int64_t* offs, const EmitTargets& t, cudaStream_t s) {
+  const int32_t cells = stencil_cells(g);
+  ensure_smem_attr((const void*)k_pair_tasks<true, K>, (int)kEmitSmem);
+  launch_pdl(k_pair_tasks<true, K>,
+             dim3(pair_grid((const void*)k_pair_tasks<true, K>, kEmitSmem)),
+             dim3(kPairWarps * 32), kEmitSmem, s, g, b, n, cells, pb, (uint32_t*)nullptr, offs, t);
+  note_launches(1);
+}
+
+}  // namespace
+
+void launch_pair_count(const GridParams& g, const GridBuffers& b, int64_t n,
+                       const GuardBand& band, uint32_t* counts, cudaStream_t s) {
+  pair_count_k<1>(g, b, n, single_band(band), counts, s);
 }
 
 void launch_pair_emit(const GridParams& g, const GridBuffers& b, int64_t n,
                       const GuardBand& band, const int64_t* offs, const EmitTargets& t,
                       cudaStream_t s) {
-  const int32_t cells = stencil_cells(g);
-  ensure_smem_attr((const void*)k_pair_tasks<true>, (int)kEmitSmem);
-  launch_pdl(k_pair_tasks<true>, dim3(pair_grid((const void*)k_pair_tasks<true>, kEmitSmem)),
-             dim3(kPairWarps * 32), kEmitSmem, s, g, b, n, cells, band, (uint32_t*)nullptr,
-             offs, t);
-  note_launches(1);
+  pair_emit_k<1>(g, b, n, single_band(band), offs, t, s);
+}
+
+void launch_pair_count_multi(const GridParams& g, const GridBuffers& b, int64_t n,
+                             const PairBands& pb, uint32_t* counts, cudaStream_t s) {
+  switch (pb.k) {
+    case 1: pair_count_k<1>(g, b, n, pb, counts, s); break;
+    case 2: pair_count_k<2>(g, b, n, pb, counts, s); break;
+    case 3: pair_count_k<3>(g, b, n, pb, counts, s); break;
+    default: pair_count_k<4>(g, b, n, pb, counts, s); break;
+  }
+  static_assert(kFp32MaxCutoffs == 4, "one instantiation per cutoff count");
+}
+
+void launch_pair_emit_multi(const GridParams& g, const GridBuffers& b, int64_t n,
+                            const PairBands& pb, const int64_t* offs, const EmitTargets& t,
+                            cudaStream_t s) {
+  switch (pb.k) {
+    case 1: pair_emit_k<1>(g, b, n, pb, offs, t, s); break;
+    case 2: pair_emit_k<2>(g, b, n, pb, offs, t, s); break;
+    case 3: pair_emit_k<3>(g, b, n, pb, offs, t, s); break;
+    default: pair_emit_k<4>(g, b, n, pb, offs, t, s); break;
+  }
 }
 
 }  // namespace nlb

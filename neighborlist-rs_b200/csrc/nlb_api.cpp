@@ -412,11 +412,13 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
     const bool same_tab = b.rank_of_bin == tab_before && tab_cap_before > 0 &&
                           c.rank_nb[0] == sp.grid.nb[0] && c.rank_nb[1] == sp.grid.nb[1] &&
                           c.rank_nb[2] == sp.grid.nb[2];
-    // One zeroed block: bin histogram, scatter cursors, pair-task counters.
-    int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 4);
+    // One zeroed block: bin histogram, scatter cursors, pair-task counters,
+    // 64-bit hit-mask cursor (8-byte aligned: 2 nb + 2 is even), build
+    // completion count.
+    int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 6);
     b.bin_count = zeroed;
     b.bin_fill = zeroed ? zeroed + nb : nullptr;
-    b.build_done = zeroed ? zeroed + 2 * nb + 2 : nullptr;
+    b.build_done = zeroed ? zeroed + 2 * nb + 4 : nullptr;
     b.bin_start = slot<int64_t>(c, kSlotBinStart, nb + 1);
     b.key = slot<uint64_t>(c, kSlotKey, n);
     b.rank = slot<int32_t>(c, kSlotRank, n);
@@ -442,23 +444,39 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
       b.irr_list = slot<int32_t>(c, kSlotIrrList, n);
       b.irr = slot<uint8_t>(c, kSlotIrr, n);
       b.counters = zeroed ? zeroed + 2 * nb : nullptr;
-      if (!b.p32 || !b.sbin || !b.groups || !b.irr_list || !b.irr || !b.counters)
+      // Hit masks of all k cutoffs, recorded by the count pass for the emit
+      // pass: the last run's need x 1.25, at least 64 words per atom and
+      // cutoff (tasks that do not fit recompute their tests in the emit).
+      const int64_t max_tasks = (n / 32 + std::min<int64_t>(n, nb) + 1) * cells;
+      int64_t mask_cap = std::max<int64_t>((int64_t)k * 64 * n + 4096,
+                                           c.pair_mask_words + c.pair_mask_words / 4);
+      const int64_t mask_have = (int64_t)(c.bufs[kSlotMasks].cap / sizeof(uint32_t));
+      if (mask_have > mask_cap) mask_cap = mask_have;
+      b.task_hdr = slot<int4>(c, kSlotTaskHdr, max_tasks);
+      b.masks = slot<uint32_t>(c, kSlotMasks, mask_cap);
+      b.mask_cap = mask_cap;
+      b.mask_top = zeroed ? reinterpret_cast<unsigned long long*>(zeroed + 2 * nb + 2) : nullptr;
+      if (!b.p32 || !b.sbin || !b.groups || !b.irr_list || !b.irr || !b.counters ||
+          !b.task_hdr || !b.masks || !b.mask_top)
         return fail(NLB_ERR_NOMEM, "device allocation failed");
     }
     if (!b.rank_of_bin || !b.bin_count || !b.bin_fill || !b.bin_start || !b.key || !b.rank ||
         !b.skey || !b.sidx || !b.skey2 || !b.sidx2 || !b.px || !b.py || !b.pz || !b.meta)
       return fail(NLB_ERR_NOMEM, "device allocation failed");
-    cudaMemsetAsync(zeroed, 0, sizeof(int32_t) * (2 * (size_t)nb + 4), s);
+    cudaMemsetAsync(zeroed, 0, sizeof(int32_t) * (2 * (size_t)nb + 6), s);
     launch_grid_build(sp.grid, d_pos, n, b, s, !same_tab);
     for (int a = 0; a < 3; ++a) c.rank_nb[a] = sp.grid.nb[a];
   }
   c.mark(1);
-  for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
+  const bool pair_tasks = sp.method == Method::kCellList && sp.fp32;
+  if (pair_tasks) {
+    sp.pbands.row = row;
+    launch_pair_count_multi(sp.grid, sp.gb, n, sp.pbands, sp.counts, s);
+  }
+  for (int32_t g0 = 0; g0 < k && !pair_tasks; g0 += kMaxCutoffsPerPass) {
     CutoffSet cs = sp.pass(g0);
     uint32_t* rows = sp.counts + (size_t)g0 * row;
-    if (sp.method == Method::kCellList && sp.fp32)
-      launch_pair_count(sp.grid, sp.gb, n, sp.band, rows, s);
-    else if (sp.method == Method::kCellList)
+    if (sp.method == Method::kCellList)
       launch_grid_count(sp.grid, sp.gb, n, cs, rows, s);
     else
       launch_brute_count(sp.brute, d_pos, n, cs, rows, s);
@@ -467,12 +485,15 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
   exclusive_scan_u32(sp.counts, (int64_t)k * row, sp.offs, scan_tmp, s);
   c.mark(3);
   // Row starts offs[q * row], q = 0..k, in one strided copy.
-  if (k + 1 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
+  if (k + 3 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
   cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), sp.offs, sizeof(int64_t) * row,
                                     sizeof(int64_t), (size_t)k + 1, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)  // the scan's bounded-wait error word
     e = cudaMemcpyAsync(c.h_small + k + 1, scan_tmp + 1, sizeof(int64_t), cudaMemcpyDeviceToHost,
                         s);
+  if (e == cudaSuccess && pair_tasks)  // hit-mask words the count pass asked for
+    e = cudaMemcpyAsync(c.h_small + k + 2, sp.gb.mask_top, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy2DAsync");
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "count pass");
@@ -482,6 +503,7 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
     c.prof_pending_count = true;
     c.harvest();
   }
+  if (pair_tasks) c.pair_mask_words = c.h_small[k + 2];
   sp.m.resize(k);
   for (int32_t q = 0; q < k; ++q) sp.m[q] = c.h_small[q + 1] - c.h_small[q];
   return Status{NLB_OK};
@@ -492,7 +514,20 @@ Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& 
                    const int64_t* base, int64_t index_offset) {
   const int32_t k = (int32_t)sp.rc_sq.size();
   c.mark(4);
-  for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
+  const bool pair_tasks = sp.method == Method::kCellList && sp.fp32;
+  if (pair_tasks) {
+    EmitTargets t;
+    std::memset(&t, 0, sizeof(t));
+    for (int32_t q = 0; q < k; ++q) {
+      t.src[q] = L.src[q];
+      t.dst[q] = L.dst[q];
+      t.sh[q] = L.sh[q];
+      t.base[q] = base[q];
+    }
+    t.index_offset = index_offset;
+    launch_pair_emit_multi(sp.grid, sp.gb, sp.n, sp.pbands, sp.offs, t, c.stream);
+  }
+  for (int32_t g0 = 0; g0 < k && !pair_tasks; g0 += kMaxCutoffsPerPass) {
     CutoffSet cs = sp.pass(g0);
     EmitTargets t;
     std::memset(&t, 0, sizeof(t));
@@ -504,9 +539,7 @@ Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& 
     }
     t.index_offset = index_offset;
     const int64_t* offs = sp.offs + (size_t)g0 * sp.row;
-    if (sp.method == Method::kCellList && sp.fp32)
-      launch_pair_emit(sp.grid, sp.gb, sp.n, sp.band, offs, t, c.stream);
-    else if (sp.method == Method::kCellList)
+    if (sp.method == Method::kCellList)
       launch_grid_emit(sp.grid, sp.gb, sp.n, cs, offs, t, c.stream);
     else
       launch_brute_emit(sp.brute, d_pos, sp.n, cs, offs, t, c.stream);
@@ -562,7 +595,23 @@ Status plan_system(const double* pos_host, int64_t n, const double* cell9, const
     for (int a = 0; a < 3; ++a)
       if (sp.grid.ns[a] < 0 || sp.grid.ns[a] > (1 << 20))
         return fail(NLB_ERR_VALUE, "stencil too large for this cutoff and cell");
-    sp.fp32 = k == 1 && fp32_search_enabled() && make_guard_band(sp.grid, rc_max, sp.band);
+    // FP32 pair tasks with a guard band per cutoff, all cutoffs in one
+    // traversal of the grid built at the largest.
+    sp.fp32 = false;
+    if (fp32_search_enabled() && k <= kFp32MaxCutoffs) {
+      PairBands pb;
+      std::memset(&pb, 0, sizeof(pb));
+      pb.k = k;
+      pb.disjoint = disjoint ? 1 : 0;
+      bool ok = true;
+      for (int32_t q = 0; q < k && ok; ++q)
+        ok = make_guard_band(sp.grid, cutoffs[sp.order[q]], pb.q[q]);
+      if (ok) {
+        sp.pbands = pb;
+        sp.band = pb.q[0];
+        sp.fp32 = true;
+      }
+    }
   } else {
     std::memcpy(sp.brute.h, sp.cell.h, sizeof(sp.brute.h));
     std::memcpy(sp.brute.hinv, sp.cell.hinv, sizeof(sp.brute.hinv));

@@ -80,6 +80,8 @@ struct Ctx {
   double prof_ms[4] = {0, 0, 0, 0};
   // Bins per axis of the rank table currently in kSlotRankTab (-1: none).
   int32_t rank_nb[3] = {-1, -1, -1};
+  // Hit-mask words the last multi-cutoff pair-task count pass needed.
+  int64_t pair_mask_words = 0;
   int64_t prof_calls = 0;
   void mark(int i) {
     if (prof) cudaEventRecord(ev[i], stream);
@@ -126,8 +128,9 @@ struct SystemPlan {
   std::vector<int32_t> order;   // sorted position q -> input cutoff index
   std::vector<double> rc_sq;    // ascending squared cutoffs
   std::vector<int64_t> m;       // edges per sorted cutoff (after count)
-  bool fp32 = false;            // single cutoff, cell list: FP32 guard-band kernels
-  GuardBand band{};
+  bool fp32 = false;            // cell list, <= kFp32MaxCutoffs: FP32 guard-band kernels
+  GuardBand band{};             // the first (or only) cutoff's band
+  PairBands pbands{};           // every sorted cutoff's band (one traversal)
   uint32_t* counts = nullptr;
   int64_t* offs = nullptr;
   int64_t row = 0;              // length of one cutoff's count row

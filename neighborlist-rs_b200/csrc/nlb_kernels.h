@@ -61,10 +61,11 @@ struct GridBuffers {
   int32_t* build_done;
   // Optional (masks == nullptr: the emit pass recomputes every test): the
   // count pass stores, per pair task, the candidate range, image shift and a
-  // 32-bit hit mask per lane per 32-candidate chunk in `masks` (bump-
-  // allocated through *mask_top, at most mask_cap words); the emit pass then
-  // only expands bits.  task_hdr[task] = {mask base (-2: nothing to emit,
-  // -1: recompute), b0, b1, packed shift}.
+  // 32-bit hit mask per lane per 32-candidate chunk per cutoff in `masks`
+  // (bump-allocated through *mask_top, at most mask_cap words; cutoff q's
+  // masks follow cutoff q - 1's); the emit pass then only expands bits.
+  // task_hdr[task] = {mask base (-2: nothing to emit, -1: recompute), b0,
+  // b1, packed shift}.
   int4* task_hdr;
   uint32_t* masks;
   unsigned long long* mask_top;
@@ -113,21 +114,31 @@ void launch_grid_count(const GridParams& g, const GridBuffers& b, int64_t n,
 void launch_grid_emit(const GridParams& g, const GridBuffers& b, int64_t n, const CutoffSet& cs,
                       const int64_t* offs, const EmitTargets& t, cudaStream_t s);
 
-// ---- k_search2.cu : single-cutoff search as (atom group, stencil cell)
-// tasks with an FP32 pair test and an exact FP64 recheck inside a guard band
-// around rc^2 (see k_search2.cu).
+// ---- k_search2.cu : stencil search as (atom group, stencil cell) tasks
+// with an FP32 pair test and an exact FP64 recheck inside a guard band
+// around each rc^2 (see k_search2.cu); one traversal serves up to
+// kFp32MaxCutoffs cutoffs.
 struct GuardBand {
   float lo;       // d2_32 < lo  => certainly inside (d2_64 < rc^2)
   float hi;       // d2_32 >= hi => certainly outside
   double rc_sq;   // exact test for d2_32 in [lo, hi)
+};
+// Cutoffs one pair-task traversal tests at once; more use the FP64 kernels.
+constexpr int32_t kFp32MaxCutoffs = 4;
+// The bands of k ascending cutoffs.  Counts and offsets hold one row of
+// `row` = n * S + 1 entries per cutoff (S = stencil cells).
+struct PairBands {
+  GuardBand q[kFp32MaxCutoffs];
+  int64_t row;
+  int32_t k;
+  int32_t disjoint;  // 1: list q leaves out the pairs inside cutoff q - 1
 };
 // Stencils above this many cells use the per-atom FP64 kernels.
 constexpr int64_t kPairMaxCells = 1024;
 // Returns false when the FP32 test cannot be made safe for this grid (the
 // band would be too wide); callers then use the FP64 kernels.
 bool make_guard_band(const GridParams& g, double rc, GuardBand& band);
-// counts[p * S + c] (S = stencil cells) for every sorted atom p and cell c,
-// plus counts[n * S] = 0.
+// counts[p * S + c] for every sorted atom p and cell c, plus counts[n * S] = 0.
 void launch_pair_count(const GridParams& g, const GridBuffers& b, int64_t n,
                        const GuardBand& band, uint32_t* counts, cudaStream_t s);
 // offs = exclusive scan of those counts; edges of (p, c) start at
@@ -135,6 +146,16 @@ void launch_pair_count(const GridParams& g, const GridBuffers& b, int64_t n,
 void launch_pair_emit(const GridParams& g, const GridBuffers& b, int64_t n,
                       const GuardBand& band, const int64_t* offs, const EmitTargets& t,
                       cudaStream_t s);
+// The same for bands.k cutoffs in one traversal: row q of counts / offs
+// (counts + q * bands.row) belongs to cutoff q, whose edges of (p, c) start
+// at t.base[q] + offs[q * row + p * S + c] - offs[q * row] in t.src[q] /
+// t.dst[q] / t.sh[q].  With b.masks set, the count pass records its hit
+// masks and the emit pass expands them.
+void launch_pair_count_multi(const GridParams& g, const GridBuffers& b, int64_t n,
+                             const PairBands& bands, uint32_t* counts, cudaStream_t s);
+void launch_pair_emit_multi(const GridParams& g, const GridBuffers& b, int64_t n,
+                            const PairBands& bands, const int64_t* offs, const EmitTargets& t,
+                            cudaStream_t s);
 
 enum BruteMode : int32_t { kBruteRaw = 0, kBruteMicMode = 1 };
 struct BruteParams {

@@ -152,6 +152,28 @@ def test_multi_cutoff_variants(nl, oracle, fixtures):
             assert_same(got[q], ref[q], f"45 cutoffs disjoint={dj} q={q}")
 
 
+@pytest.mark.parametrize("disjoint", [False, True])
+def test_multi_guard_band_shell_edges(nl, oracle, disjoint):
+    """Lattice pairs exactly on each cutoff of a multi-cutoff request (and one
+    ulp either side): every per-cutoff FP32 pass must defer the undecidable
+    pairs, including those on the inner edge of a disjoint shell."""
+    a = 2.0
+    g = np.arange(10) * a
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    cell = nl.PyCell(eye(20.0).tolist())
+    up, dn = np.nextafter(1.0, 2.0), np.nextafter(1.0, 0.0)
+    sets = [[2.0, np.sqrt(8.0), np.sqrt(12.0), 4.0],
+            [2.0 * up, np.sqrt(8.0) * dn, 4.0 * up],
+            [4.0, 2.0, np.sqrt(8.0)]]
+    for cs in sets:
+        cs = [float(c) for c in cs]
+        for p in (pos, pos + 0.5):
+            got = nl.build_neighborlists_multi(cell, p, cs, disjoint=disjoint)
+            ref = oracle.search_single_multi(p, eye(20.0), PBC3, cs, disjoint=disjoint, nthreads=8)
+            for q in range(len(cs)):
+                assert_same(got[q], ref[q], f"lattice multi {cs} disjoint={disjoint} q={q}")
+
+
 def test_multi_brute_and_labels(nl, oracle):
     pos = np.array([[0.0, 0, 0], [1.0, 0, 0], [2.5, 0, 0]])
     got = nl.build_neighborlists_multi(None, pos, [1.6, 3.0], labels=["s", "l"])
