@@ -77,10 +77,24 @@ def _case_device(rc):
     return run
 
 
+def settle_batch_tuner(nl, fn, limit=64):
+    """Calls fn() until the launch-shape tuner has chosen a shape for every
+    kind of batch fn issues (the batched path's steady state); returns the
+    chosen shapes."""
+    for _ in range(limit):
+        fn()
+        state = nl.batch_tuner_state()
+        if state and all(e["shape"] >= 0 for e in state):
+            break
+    return [dict(e, **nl.batch_shape_info(e["shape"])) for e in nl.batch_tuner_state()
+            if e["shape"] >= 0]
+
+
 def _case_batch(nl, torch, steps, warmup):
     from neighborlist_rs import workloads as W
 
     pb, bb, cb = W.concat_batch(W.uneven_batch())
+    settle_batch_tuner(nl, lambda: nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0))
     for _ in range(warmup):
         nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0)
     t0 = time.perf_counter()
@@ -493,6 +507,9 @@ def extra_measurements(nl, torch, args):
     # batched uneven systems (host-buffer call) vs the plain per-system loop
     systems = W.uneven_batch()
     pb, bb, cb = W.concat_batch(systems)
+    nl.batch_tuner_reset()
+    shapes = settle_batch_tuner(
+        nl, lambda: nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0))
     nl.profile(True)
     tb, rb = median_call(lambda: nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0))
     calls, ph = nl.profile_read()
@@ -509,7 +526,7 @@ def extra_measurements(nl, torch, args):
         "ms_per_call_e2e": 1e3 * tb, "systems_per_s_device": len(systems) / (dev_ms * 1e-3),
         "device_ms_phases": {k: v / max(calls, 1) for k, v in ph.items()},
         "plain_per_system_loop_systems_per_s": sample / tp,
-        "atoms": int(pb.shape[0]), "edges": mb}
+        "atoms": int(pb.shape[0]), "edges": mb, "tuned_launch_shape": shapes}
     out["served"] = served_measurements(nl)
     out["output_options_rc6"] = output_option_measurements(nl, torch)
     out["verlet_md_rc6"] = verlet_measurements(nl, torch)
@@ -657,7 +674,7 @@ def run_stream_raw(srv, reqs, device=False):
 
 
 def served_measurements(nl):
-    """Served loop (continuous batching, 40 GB HBM budget): a small-request
+    """Served loop (continuous batching, 40 GB HBM budget, 4 workers): a small-request
     mix and a bounded sample of the full request-size distribution, each
     against the plain per-request loop (build_neighborlists) over the same
     requests.  Every arm runs once untimed over the same requests first."""
@@ -682,7 +699,7 @@ def served_measurements(nl):
     small = as_reqs(W.request_stream(4096, seed=21, n_range=(16, 2048)))
     plain(small[:1024])
     res = {"plain_per_request_loop": plain(small[:1024])}
-    with Server(hbm_budget_bytes=40 << 30, workers=2, max_batch=4096) as srv:
+    with Server(hbm_budget_bytes=40 << 30, workers=4, max_batch=4096) as srv:
         run_stream(srv, small, None)
         res["saturated_python_api"] = run_stream(srv, small, None)
         res["saturated_c_abi"] = run_stream_raw(srv, small)
@@ -700,7 +717,7 @@ def served_measurements(nl):
     full = as_reqs(W.request_stream(48, seed=22))
     plain(full)
     res = {"plain_per_request_loop": plain(full)}
-    with Server(hbm_budget_bytes=40 << 30, workers=2, max_batch=4096) as srv:
+    with Server(hbm_budget_bytes=40 << 30, workers=4, max_batch=4096) as srv:
         # Each worker grows its workspace (a device-synchronising reallocation)
         # the first time it meets a larger request, and results of new sizes
         # take new pinned blocks: warm every path until that has settled.

@@ -137,6 +137,29 @@ int64_t nlb_kernel_launches(void);
 void nlb_profile(int enable);
 int64_t nlb_profile_read(double* ms);
 
+/* Launch shapes of the batched kernels (no counterpart in the reference,
+ * whose batch path has no launch configuration).  Batches are tuned per kind
+ * (cutoff count, power-of-two buckets of the system count, the largest and
+ * the mean system, quarter-octave bucket of the largest cutoff): the first
+ * batch of a kind runs its count pass once in every candidate shape, timed
+ * with CUDA events, and the kind keeps the fastest.  Every shape gives
+ * identical results.
+ *
+ * nlb_batch_shape(i) pins shape i (0 = the default) for every batched
+ * launch of the process, -1 returns to tuning; it returns the number of
+ * shapes, or -1 if i is out of range.  NLB_BATCH_SHAPE=i in the environment
+ * pins from the start.  nlb_batch_shape_info fills {threads per CTA for
+ * whole systems, threads per CTA for split systems, atoms per work item of a
+ * split system, size above which a system is split}.  nlb_batch_tuner_state
+ * writes up to cap rows of 8 int64 {device, cutoffs (0: one per system),
+ * log2 systems, log2 largest, log2 mean, cutoff bucket, chosen shape (-1:
+ * not decided), candidate shapes} and returns the number of kinds seen;
+ * nlb_batch_tuner_reset forgets them. */
+int32_t nlb_batch_shape(int32_t shape);
+int32_t nlb_batch_shape_info(int32_t shape, int32_t* out4);
+int32_t nlb_batch_tuner_state(int64_t* out, int32_t cap);
+void nlb_batch_tuner_reset(void);
+
 /* ---- Output options (asked for by the reference's spec.md:100-108 and
  * RUST_API.md:89-90, not implemented by the reference). ----
  * nlb_build_ex: the nlb_build search, then on the device:

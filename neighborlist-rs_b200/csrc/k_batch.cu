@@ -28,10 +28,6 @@ namespace nlb {
 
 namespace {
 
-constexpr int kBatchThreads = 256;       // CTA size for systems of <= kBatchLargeAtoms
-constexpr int kBatchLargeThreads = 512;  // CTA size for larger systems
-constexpr int kBatchChunk = 256;         // atoms per work item of a larger system
-
 __device__ __forceinline__ double dfmin(double a, double b) {
   if (a != a) return b;
   if (b != b) return a;
@@ -452,9 +448,10 @@ __device__ __forceinline__ void system_cutoff(const CutoffSet& cs, const SysPlan
 }
 
 template <int THREADS>
-// The 512-thread count spills at the default 64-register budget; one CTA per
-// SM with room for ~106 registers measured 7-8 % faster.
-__global__ void __launch_bounds__(THREADS, THREADS >= 512 ? 1 : 3)
+// 80 registers per thread for 64 / 128 / 256-thread CTAs.  The 512-thread count
+// spills at the 64-register budget of two CTAs per SM; one CTA per SM with
+// room for ~106 registers measured 7-8 % faster.
+__global__ void __launch_bounds__(THREADS, THREADS >= 512 ? 1 : 768 / THREADS)
     k_batch_count(const SysPlan* __restrict__ plans, const int2* __restrict__ items, int n_items,
                   int chunk, const double* __restrict__ pos, int cap, CutoffSet cs,
                   uint32_t* __restrict__ counts, int64_t row, int* __restrict__ work) {
@@ -594,25 +591,68 @@ void launch_sys_bounds(const SysPlan* plans, int n_sys, const int64_t* offs, int
   note_launches(1);
 }
 
+const BatchShape kBatchShapeTable[kBatchShapes] = {
+    // small_threads, large_threads, chunk, large_atoms
+    {256, 512, 256, 512},  // default
+    {128, 512, 256, 512},  // more systems in flight per SM
+    {256, 256, 128, 256},  // finer items for the mid-size systems
+    {128, 256, 128, 256},
+    {256, 512, 128, 512},
+    {512, 512, 256, 1024},  // systems up to 1024 atoms whole
+    {64, 512, 256, 512},    // two warps per system: tiny systems
+};
+
+namespace {
+
+using CountFn = decltype(&k_batch_count<256>);
+using EmitFn = decltype(&k_batch_emit<256>);
+
+CountFn count_fn(int threads) {
+  return threads <= 64    ? &k_batch_count<64>
+         : threads <= 128 ? &k_batch_count<128>
+         : threads <= 256 ? &k_batch_count<256>
+                          : &k_batch_count<512>;
+}
+EmitFn emit_fn(int threads) {
+  return threads <= 64    ? &k_batch_emit<64>
+         : threads <= 128 ? &k_batch_emit<128>
+         : threads <= 256 ? &k_batch_emit<256>
+                          : &k_batch_emit<512>;
+}
+
+}  // namespace
+
+void preload_batch_kernels() {
+  // Loading a kernel's module happens on its first launch unless something
+  // asks for its attributes first (lazy loading): do it for every variant.
+  cudaFuncAttributes a;
+  for (int threads : {64, 128, 256, 512}) {
+    cudaFuncGetAttributes(&a, (const void*)count_fn(threads));
+    cudaFuncGetAttributes(&a, (const void*)emit_fn(threads));
+  }
+  cudaGetLastError();
+}
+
 void launch_batch_count(const SysPlan* plans, const BatchItems& w, const double* pos,
                         const CutoffSet& cs, uint32_t* counts, int64_t row, int* work2,
                         cudaStream_t s) {
+  const BatchShape& sh = w.shape;
   if (w.n_large > 0) {
     const size_t smem = batch_smem_bytes(w.cap_large);
-    auto k = k_batch_count<kBatchLargeThreads>;
+    const CountFn k = count_fn(sh.large_threads);
     ensure_smem_attr((const void*)k, (int)smem);
-    const int grid = std::min(grid_for((const void*)k, kBatchLargeThreads, smem), w.n_large);
-    k<<<grid, kBatchLargeThreads, smem, s>>>(plans, w.items, w.n_large, kBatchChunk, pos,
-                                             w.cap_large, cs, counts, row, work2);
+    const int grid = std::min(grid_for((const void*)k, sh.large_threads, smem), w.n_large);
+    k<<<grid, sh.large_threads, smem, s>>>(plans, w.items, w.n_large, sh.chunk, pos,
+                                           w.cap_large, cs, counts, row, work2);
     note_launches(1);
   }
   if (w.n_small > 0) {
     const size_t smem = batch_smem_bytes(w.cap_small);
-    auto k = k_batch_count<kBatchThreads>;
+    const CountFn k = count_fn(sh.small_threads);
     ensure_smem_attr((const void*)k, (int)smem);
-    const int grid = std::min(grid_for((const void*)k, kBatchThreads, smem), w.n_small);
-    k<<<grid, kBatchThreads, smem, s>>>(plans, w.items + w.n_large, w.n_small, 1 << 30, pos,
-                                        w.cap_small, cs, counts, row, work2 + 1);
+    const int grid = std::min(grid_for((const void*)k, sh.small_threads, smem), w.n_small);
+    k<<<grid, sh.small_threads, smem, s>>>(plans, w.items + w.n_large, w.n_small, 1 << 30, pos,
+                                           w.cap_small, cs, counts, row, work2 + 1);
     note_launches(1);
   }
 }
@@ -620,45 +660,48 @@ void launch_batch_count(const SysPlan* plans, const BatchItems& w, const double*
 void launch_batch_emit(const SysPlan* plans, const BatchItems& w, const double* pos,
                        const CutoffSet& cs, const int64_t* offs, int64_t row,
                        const EmitTargets& t, int* work2, cudaStream_t s) {
+  const BatchShape& sh = w.shape;
   if (w.n_large > 0) {
     const size_t smem = batch_smem_bytes(w.cap_large);
-    auto k = k_batch_emit<kBatchLargeThreads>;
+    const EmitFn k = emit_fn(sh.large_threads);
     ensure_smem_attr((const void*)k, (int)smem);
-    const int grid = std::min(grid_for((const void*)k, kBatchLargeThreads, smem), w.n_large);
-    k<<<grid, kBatchLargeThreads, smem, s>>>(plans, w.items, w.n_large, kBatchChunk, pos,
-                                             w.cap_large, cs, offs, row, t, work2);
+    const int grid = std::min(grid_for((const void*)k, sh.large_threads, smem), w.n_large);
+    k<<<grid, sh.large_threads, smem, s>>>(plans, w.items, w.n_large, sh.chunk, pos,
+                                           w.cap_large, cs, offs, row, t, work2);
     note_launches(1);
   }
   if (w.n_small > 0) {
     const size_t smem = batch_smem_bytes(w.cap_small);
-    auto k = k_batch_emit<kBatchThreads>;
+    const EmitFn k = emit_fn(sh.small_threads);
     ensure_smem_attr((const void*)k, (int)smem);
-    const int grid = std::min(grid_for((const void*)k, kBatchThreads, smem), w.n_small);
-    k<<<grid, kBatchThreads, smem, s>>>(plans, w.items + w.n_large, w.n_small, 1 << 30, pos,
-                                        w.cap_small, cs, offs, row, t, work2 + 1);
+    const int grid = std::min(grid_for((const void*)k, sh.small_threads, smem), w.n_small);
+    k<<<grid, sh.small_threads, smem, s>>>(plans, w.items + w.n_large, w.n_small, 1 << 30, pos,
+                                           w.cap_small, cs, offs, row, t, work2 + 1);
     note_launches(1);
   }
 }
 
-void plan_batch_items(const int64_t* sizes, int n_sys, std::vector<int2>& items, BatchItems& w) {
+void plan_batch_items(const int64_t* sizes, int n_sys, const BatchShape& shape,
+                      std::vector<int2>& items, BatchItems& w) {
   std::vector<int32_t> order(n_sys);
   for (int i = 0; i < n_sys; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(),
                    [&](int32_t x, int32_t y) { return sizes[x] > sizes[y]; });
   items.clear();
   w = BatchItems{};
+  w.shape = shape;
   int64_t max_large = 0, max_small = 0;
   for (int32_t i : order) {
     const int64_t n = sizes[i];
-    if (n > kBatchLargeAtoms) {
-      for (int64_t a = 0; a < n; a += kBatchChunk) items.push_back(make_int2(i, (int)a));
+    if (n > shape.large_atoms) {
+      for (int64_t a = 0; a < n; a += shape.chunk) items.push_back(make_int2(i, (int)a));
       max_large = std::max(max_large, n);
     }
   }
   w.n_large = (int)items.size();
   for (int32_t i : order) {
     const int64_t n = sizes[i];
-    if (n <= kBatchLargeAtoms) {
+    if (n <= shape.large_atoms) {
       items.push_back(make_int2(i, 0));
       max_small = std::max(max_small, n);
     }

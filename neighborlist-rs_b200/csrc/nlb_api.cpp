@@ -315,6 +315,7 @@ void release_thread_ctx() {
       if (b.p) cudaFree(b.p);
     for (cudaEvent_t ev : c->ev)
       if (ev) cudaEventDestroy(ev);
+    tune_release(*c);
     if (c->h_small) cudaFreeHost(c->h_small);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     cudaSetDevice(prev);

@@ -95,32 +95,37 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
   // persistent CTAs (larger systems split into chunks of atoms).
   std::vector<int64_t> sizes(ns);
   for (int32_t i = 0; i < ns; ++i) sizes[i] = starts[a + i + 1] - starts[a + i];
-  std::vector<int2> items;
-  BatchItems bw;
-  plan_batch_items(sizes.data(), ns, items, bw);
+  // (every candidate launch shape when this kind of batch is new)
+  ShapeTrials trials;
+  Status st = trials.prepare(c, make_tune_key(c.device, k, sizes.data(), ns, rc_max),
+                             sizes.data(), ns, kSlotBatch0 + 1);
+  if (!st.ok()) return st;
 
   SysPlan* plans = slot<SysPlan>(c, kSlotBatch0 + 0, ns);
-  int2* items_d = slot<int2>(c, kSlotBatch0 + 1, items.size());
   int32_t* flags = slot<int32_t>(c, kSlotBatch0 + 2, 3);  // [0] plan error, [1..2] work counters
   uint32_t* counts = slot<uint32_t>(c, kSlotBatch0 + 3, (size_t)k * row);
   int64_t* offs = slot<int64_t>(c, kSlotBatch0 + 4, (size_t)k * row + 1);
   int64_t* scan_tmp = slot<int64_t>(c, kSlotBatch0 + 5, scan_tmp_elems((int64_t)k * row));
-  if (!plans || !items_d || !flags || !counts || !offs || !scan_tmp)
+  if (!plans || !flags || !counts || !offs || !scan_tmp)
     return fail(NLB_ERR_NOMEM, "device allocation failed");
-  bw.items = items_d;
 
-  cudaMemcpyAsync(items_d, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s);
   cudaMemsetAsync(flags, 0, sizeof(int32_t) * 3, s);
   cudaMemsetAsync(counts, 0, sizeof(uint32_t) * (size_t)k * row, s);
   c.mark(0);
   launch_plan(d_pos, d_starts, a, b, d_cells, d_pbcs, d_has, rc_max, g_bf_threshold.load(),
               multi ? 1 : 0, run_start, plans, flags, s);
   c.mark(1);
-  for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
-    const CutoffSet cs = make_pass(rc_sq, g0, disjoint);
-    cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
-    launch_batch_count(plans, bw, d_pos, cs, counts + (size_t)g0 * row, row, flags + 1, s);
+  // (The counts are the same in every shape: each trial writes all of them.)
+  for (size_t t = 0; t < trials.w.size(); ++t) {
+    trials.mark(c, t);
+    for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
+      const CutoffSet cs = make_pass(rc_sq, g0, disjoint);
+      cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
+      launch_batch_count(plans, trials.w[t], d_pos, cs, counts + (size_t)g0 * row, row,
+                         flags + 1, s);
+    }
   }
+  trials.mark(c, trials.w.size());
   c.mark(2);
   exclusive_scan_u32(counts, (int64_t)k * row, offs, scan_tmp, s);
   c.mark(3);
@@ -147,6 +152,7 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
   for (int32_t q = 0; q < k; ++q) m[q] = c.h_small[q + 1] - c.h_small[q];
   if (!out.reserve(m, s)) return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
 
+  const BatchItems& bw = trials.pick(c);
   c.mark(4);
   for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
     const CutoffSet cs = make_pass(rc_sq, g0, disjoint);

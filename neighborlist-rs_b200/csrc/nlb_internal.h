@@ -58,6 +58,16 @@ enum Slot : int {
 
 constexpr int kSmallHost = 4096;  // int64 slots of the per-context pinned scratch
 
+// Kind of batch the launch-shape tuner keys on: cutoff count (0: one cutoff
+// per system), and power-of-two buckets of the system count, the largest and
+// the mean system, and a quarter-octave bucket of the largest cutoff.
+struct TuneKey {
+  int32_t device, k, n_sys_log2, max_log2, mean_log2, rc_bucket;
+  bool operator<(const TuneKey& o) const;
+};
+TuneKey make_tune_key(int32_t device, int32_t k, const int64_t* sizes, int32_t n_sys,
+                      double rc_max);
+
 struct Ctx {
   struct Buf {
     void* p = nullptr;
@@ -82,6 +92,9 @@ struct Ctx {
   int32_t rank_nb[3] = {-1, -1, -1};
   // Hit-mask words the last multi-cutoff pair-task count pass needed.
   int64_t pair_mask_words = 0;
+  // Events timing the candidate launch shapes of a new kind of batch
+  // (nlb_tune.cpp), created on first use.
+  cudaEvent_t tune_ev[kBatchShapes + 1] = {};
   int64_t prof_calls = 0;
   void mark(int i) {
     if (prof) cudaEventRecord(ev[i], stream);
@@ -171,6 +184,24 @@ void zero_results(nlb_result* outs, int32_t k);
 Status empty_results(nlb_result* outs, int32_t k);
 bool cutoffs_valid(const double* cs, int32_t k);
 Status upload_positions(Ctx& c, const double* pos, int64_t n, double** d_pos);
+
+// ---- launch-shape tuner for the batched kernels (nlb_tune.cpp)
+// The work items of one batched run in every launch shape it tries: the
+// chosen (or pinned) shape of its kind, or, for the first batch of a new
+// kind, every candidate shape.  Usage: prepare() before the count pass; for
+// each i < w.size(), mark(i) then that shape's count launches; mark(w.size());
+// after the host has synchronised on the count pass, pick() returns the
+// items for the emit pass (the fastest count, remembered for the kind).
+struct ShapeTrials {
+  TuneKey key{};
+  std::vector<int32_t> shapes;
+  std::vector<BatchItems> w;
+  bool timed = false;
+  Status prepare(Ctx& c, const TuneKey& k, const int64_t* sizes, int32_t n_sys, int items_slot);
+  void mark(Ctx& c, size_t i);
+  const BatchItems& pick(Ctx& c);
+};
+void tune_release(Ctx& c);
 
 Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_batch,
                  const double* cutoffs, int32_t k, const double* cells, const uint8_t* pbcs,

@@ -194,18 +194,36 @@ void launch_plan(const double* pos, const int64_t* starts, int32_t s0, int32_t s
 // out[s] = first edge of system s relative to the run (k == 1 rows), out[ns] = total.
 void launch_sys_bounds(const SysPlan* plans, int n_sys, const int64_t* offs, int64_t row,
                        int64_t* out, cudaStream_t s);
-// Work items of one batched pass: (system, first atom) pairs, systems with
-// more than kBatchLargeAtoms atoms first (split into chunks, 512-thread CTAs),
-// then the smaller ones (one item each, 256-thread CTAs), each group largest
-// first.  cap_* = power of two >= the largest system of the group.
-constexpr int kBatchLargeAtoms = 512;
+// Launch shape of the batched kernels: the systems of at most large_atoms
+// atoms are one work item each, run by CTAs of small_threads; larger systems
+// are split into work items of `chunk` atoms run by CTAs of large_threads.
+// Every shape gives the same results (counts per atom, offsets from one
+// scan); which is fastest depends on the mix, so the tuner (nlb_tune.cpp)
+// picks one per kind of batch.  Cell size is not a free parameter: the bins
+// of the cell list fix the output order.
+struct BatchShape {
+  int small_threads;  // 64, 128, 256 or 512
+  int large_threads;  // 256 or 512
+  int chunk;          // atoms per work item of a large system
+  int large_atoms;    // systems above this many atoms are split
+};
+constexpr int kBatchShapes = 7;
+extern const BatchShape kBatchShapeTable[kBatchShapes];  // [0]: the default
+// Loads every batched kernel variant into the current device's context, so
+// that no variant's first launch pays for loading its module.
+void preload_batch_kernels();
+// Work items of one batched pass: (system, first atom) pairs, the split
+// (large) systems first, then the others, each group largest first.
+// cap_* = power of two >= the largest system of the group.
 struct BatchItems {
   const int2* items = nullptr;  // device: [n_large | n_small]
   int n_large = 0, n_small = 0;
   int cap_large = 32, cap_small = 32;
+  BatchShape shape{256, 512, 256, 512};
 };
 // Host: builds the item list (upload it and set w.items before launching).
-void plan_batch_items(const int64_t* sizes, int n_sys, std::vector<int2>& items, BatchItems& w);
+void plan_batch_items(const int64_t* sizes, int n_sys, const BatchShape& shape,
+                      std::vector<int2>& items, BatchItems& w);
 // counts[q * row + slot + p]; work2[0..1] must be zero on entry.
 void launch_batch_count(const SysPlan* plans, const BatchItems& w, const double* pos,
                         const CutoffSet& cs, uint32_t* counts, int64_t row, int* work2,

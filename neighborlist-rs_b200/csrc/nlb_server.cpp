@@ -570,22 +570,24 @@ class Server {
 
     const int64_t row = total_atoms + 1;
     std::vector<int64_t> sizes(ns);
-    for (int32_t i = 0; i < ns; ++i) sizes[i] = items[i]->n;
-    std::vector<int2> work_items;
-    BatchItems bw;
-    plan_batch_items(sizes.data(), ns, work_items, bw);
+    double rc_max = 0.0;
+    for (int32_t i = 0; i < ns; ++i) {
+      sizes[i] = items[i]->n;
+      rc_max = std::max(rc_max, items[i]->rc);
+    }
+    // (every candidate launch shape when this kind of batch is new)
+    ShapeTrials trials;
+    st = trials.prepare(*c, make_tune_key(c->device, 0, sizes.data(), ns, rc_max), sizes.data(),
+                        ns, kSlotBatch0 + 1);
+    if (!st.ok()) return st;
     SysPlan* plans = slot<SysPlan>(*c, kSlotBatch0 + 0, ns);
-    int2* items_d = slot<int2>(*c, kSlotBatch0 + 1, work_items.size());
     int32_t* flags = slot<int32_t>(*c, kSlotBatch0 + 2, 3);
     uint32_t* counts = slot<uint32_t>(*c, kSlotBatch0 + 3, row);
     int64_t* offs = slot<int64_t>(*c, kSlotBatch0 + 4, row + 1);
     int64_t* scan_tmp = slot<int64_t>(*c, kSlotBatch0 + 5, scan_tmp_elems(row));
     int64_t* bounds = slot<int64_t>(*c, kSlotBatch0 + 11, ns + 1);
-    if (!plans || !items_d || !flags || !counts || !offs || !scan_tmp || !bounds)
+    if (!plans || !flags || !counts || !offs || !scan_tmp || !bounds)
       return fail(NLB_ERR_NOMEM, "device allocation failed");
-    bw.items = items_d;
-    cudaMemcpyAsync(items_d, work_items.data(), sizeof(int2) * work_items.size(),
-                    cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(flags, 0, sizeof(int32_t) * 3, s);
     cudaMemsetAsync(counts, 0, sizeof(uint32_t) * row, s);
     launch_plan(d_pos, d_starts, 0, ns, d_cells, d_pbc, d_has, 0.0, g_bf_threshold.load(), 0, 0,
@@ -593,7 +595,13 @@ class Server {
     CutoffSet cs;
     std::memset(&cs, 0, sizeof(cs));
     cs.k = 0;  // per-system cutoffs
-    launch_batch_count(plans, bw, d_pos, cs, counts, row, flags + 1, s);
+    // (The counts are the same in every shape: each trial writes all of them.)
+    for (size_t t = 0; t < trials.w.size(); ++t) {
+      trials.mark(*c, t);
+      if (t > 0) cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
+      launch_batch_count(plans, trials.w[t], d_pos, cs, counts, row, flags + 1, s);
+    }
+    trials.mark(*c, trials.w.size());
     exclusive_scan_u32(counts, row, offs, scan_tmp, s);
     launch_sys_bounds(plans, ns, offs, row, bounds, s);
     // System bounds, the plan error word and the scan's bounded-wait error
@@ -644,7 +652,7 @@ class Server {
     t.local_indices = 1;
     t.system_blocks = 1;  // request i: [src | dst] at src + 2 hb[i]
     cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
-    launch_batch_emit(plans, bw, d_pos, cs, offs, row, t, flags + 1, s);
+    launch_batch_emit(plans, trials.pick(*c), d_pos, cs, offs, row, t, flags + 1, s);
     // Host results of the batch come back in two copies into shared pinned
     // blocks, each request holding slices of them.
     bool any_host = false;

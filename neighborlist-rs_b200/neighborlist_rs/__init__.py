@@ -16,7 +16,6 @@ from __future__ import annotations
 import ctypes
 import math
 import os
-import weakref
 
 import numpy as np
 
@@ -81,20 +80,38 @@ def _check(code: int) -> None:
     raise RuntimeError(f"neighborlist_rs (CUDA): {msg}")
 
 
-def _arr(ptr, count, ctype, dtype):
+class _HostBlock:
+    """Owner of one library-allocated host block, exposed to numpy through
+    the array interface (the array's base); the block is returned to the
+    library when the last view is gone.  (A ctypes array type per length
+    would cost ~20 us per result and grow ctypes' type cache.)"""
+
+    __slots__ = ("__array_interface__", "_ptr")
+
+    def __init__(self, ptr, count, typestr):
+        self._ptr = ptr
+        self.__array_interface__ = {"data": (ptr, False), "shape": (count,),
+                                    "typestr": typestr, "version": 3}
+
+    def __del__(self):
+        try:
+            _lib.nlb_host_free(ctypes.c_void_p(self._ptr))
+        except Exception:  # interpreter shutdown
+            pass
+
+
+def _arr(ptr, count, dtype):
     """numpy view of `count` library-owned elements; freed with the array."""
     if count == 0:
         _lib.nlb_host_free(ptr)
         return np.zeros(0, dtype=dtype)
-    buf = (ctype * count).from_address(ptr)
-    weakref.finalize(buf, _lib.nlb_host_free, ctypes.c_void_p(ptr))
-    return np.frombuffer(buf, dtype=dtype)
+    return np.asarray(_HostBlock(ptr, count, np.dtype(dtype).str))
 
 
 def _to_dict(r: _Result) -> dict:
     m = int(r.n_edges)
-    ei = _arr(r.edge_index, 2 * m, ctypes.c_int64, np.int64).reshape(2, m)
-    sh = _arr(r.shift, 3 * m, ctypes.c_int32, np.int32).reshape(m, 3)
+    ei = _arr(r.edge_index, 2 * m, np.int64).reshape(2, m)
+    sh = _arr(r.shift, 3 * m, np.int32).reshape(m, 3)
     return {"edge_index": ei, "shift": sh}
 
 
@@ -410,6 +427,60 @@ _lib.nlb_kernel_launches.restype = ctypes.c_int64
 _lib.nlb_profile.argtypes = [ctypes.c_int]
 _lib.nlb_profile_read.argtypes = [_dp]
 _lib.nlb_profile_read.restype = ctypes.c_int64
+_lib.nlb_batch_shape.argtypes = [ctypes.c_int32]
+_lib.nlb_batch_shape.restype = ctypes.c_int32
+_lib.nlb_batch_shape_info.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+_lib.nlb_batch_shape_info.restype = ctypes.c_int32
+_lib.nlb_batch_tuner_state.argtypes = [ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]
+_lib.nlb_batch_tuner_state.restype = ctypes.c_int32
+_lib.nlb_batch_tuner_reset.argtypes = []
+_lib.nlb_batch_tuner_reset.restype = None
+
+
+_lib.nlb_pinned_stats.argtypes = [ctypes.POINTER(ctypes.c_int64)]
+_lib.nlb_pinned_stats.restype = None
+_PINNED_STATS = ("host_alloc_calls", "host_alloc_us", "host_alloc_bytes", "host_free_calls",
+                 "host_free_us", "cache_hits", "cached_bytes")
+
+
+def pinned_stats() -> dict:
+    """Counters of the pinned host pool behind every host result."""
+    buf = (ctypes.c_int64 * len(_PINNED_STATS))()
+    _lib.nlb_pinned_stats(buf)
+    return dict(zip(_PINNED_STATS, (int(x) for x in buf)))
+
+
+def set_batch_shape(shape: int | None) -> int:
+    """Pin launch shape `shape` of the batched kernels (None: tune per kind of
+    batch, the default).  Returns the number of shapes."""
+    r = int(_lib.nlb_batch_shape(-1 if shape is None else int(shape)))
+    if r < 0:
+        raise ValueError(f"no batch launch shape {shape}")
+    return r
+
+
+def batch_shape_info(shape: int) -> dict:
+    """{small_threads, large_threads, chunk, large_atoms} of launch shape `shape`."""
+    out = (ctypes.c_int32 * 4)()
+    if _lib.nlb_batch_shape_info(int(shape), out) != 0:
+        raise ValueError(f"no batch launch shape {shape}")
+    return dict(zip(("small_threads", "large_threads", "chunk", "large_atoms"), list(out)))
+
+
+def batch_tuner_state() -> list:
+    """One dict per kind of batch seen: its key, the chosen shape (-1: not
+    decided yet) and the number of candidate shapes it was timed in."""
+    n = int(_lib.nlb_batch_tuner_state(None, 0))
+    buf = np.zeros(8 * max(n, 1), np.int64)
+    n = min(n, int(_lib.nlb_batch_tuner_state(buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), n)))
+    keys = ("device", "cutoffs", "systems_log2", "max_atoms_log2", "mean_atoms_log2",
+            "cutoff_bucket", "shape", "candidates")
+    return [dict(zip(keys, (int(v) for v in buf[8 * i:8 * i + 8]))) for i in range(n)]
+
+
+def batch_tuner_reset() -> None:
+    """Forget every tuned kind of batch (the next calls tune again)."""
+    _lib.nlb_batch_tuner_reset()
 
 
 def set_stream(stream_handle: int | None) -> None:
@@ -531,12 +602,12 @@ def build_neighborlists_ex(cell, positions, cutoff, directed=False, vectors=Fals
     _check(_lib.nlb_build_ex(pos.ctypes.data_as(_dp), n, c, h, pb,
                              _ex_flags(directed, vectors, distances), ctypes.byref(r)))
     m = int(r.n_edges)
-    out = {"edge_index": _arr(r.edge_index, 2 * m, ctypes.c_int64, np.int64).reshape(2, m),
-           "shift": _arr(r.shift, 3 * m, ctypes.c_int32, np.int32).reshape(m, 3)}
+    out = {"edge_index": _arr(r.edge_index, 2 * m, np.int64).reshape(2, m),
+           "shift": _arr(r.shift, 3 * m, np.int32).reshape(m, 3)}
     if vectors:
-        out["vectors"] = _arr(r.vectors, 3 * m, ctypes.c_double, np.float64).reshape(m, 3)
+        out["vectors"] = _arr(r.vectors, 3 * m, np.float64).reshape(m, 3)
     if distances:
-        out["distances"] = _arr(r.distances, m, ctypes.c_double, np.float64)
+        out["distances"] = _arr(r.distances, m, np.float64)
     return out
 
 

@@ -394,6 +394,33 @@ def test_non_finite_positions(nl, oracle, cell):
     assert_same(got, ref, f"non-finite positions (cell={cell})")
 
 
+def test_result_arrays_own_their_pinned_blocks(nl):
+    """Result arrays view library-owned pinned blocks: a view outliving its
+    dict keeps the block (and its values); dropped results return their
+    blocks, so steady-state calls allocate no new pinned memory."""
+    from neighborlist_rs import workloads as W
+
+    pos, rows = W.cluster_liquid(n_clusters=139, box=23.2, seed=21)
+    cell = nl.PyCell(rows.T.tolist())
+    first = nl.build_neighborlists(cell, pos, 6.0)
+    ref_ei, ref_sh = first["edge_index"].copy(), first["shift"].copy()
+    view = first["edge_index"][:, ::7]
+    del first
+    for _ in range(3):
+        nl.build_neighborlists(cell, pos, 6.0)
+    s0 = nl.pinned_stats()
+    for _ in range(20):
+        r = nl.build_neighborlists(cell, pos, 6.0)
+        assert r["edge_index"].base is not None and not r["edge_index"].flags.owndata
+        del r
+    s1 = nl.pinned_stats()
+    assert s1["host_alloc_calls"] == s0["host_alloc_calls"], (s0, s1)
+    assert s1["cache_hits"] >= s0["cache_hits"] + 20, (s0, s1)
+    assert np.array_equal(view, ref_ei[:, ::7])
+    r = nl.build_neighborlists(cell, pos, 6.0)
+    assert_same(r, (ref_ei, ref_sh), "after block reuse")
+
+
 def test_concurrent_host_threads(nl):
     """Builds from several host threads at once (each thread has its own
     stream and workspace) give the single-threaded results."""
