@@ -41,9 +41,15 @@ namespace {
 
 constexpr int kPairWarps = 8;  // warps per CTA
 // Emit pass: hits of one task staged per warp before the warp writes them out
-// (dynamic shared memory, kPairWarps x kStageCap words).
-constexpr int kStageCap = 1536;
-constexpr size_t kEmitSmem = sizeof(uint32_t) * kPairWarps * kStageCap;
+// (dynamic shared memory, kPairWarps x stage_cap 16-bit entries: lane << 11 |
+// candidate offset, for cells of at most kStageCell candidates).  Grids whose
+// tasks hold at most ~kStageSmall hits get the small stage; denser ones the
+// large (88 KB, so that two 256-thread CTAs still fit an SM beside their
+// static shared memory), which the small-task grids would pay for in L1.
+constexpr int kStageSmall = 1536;
+constexpr int kStageLarge = 5632;
+constexpr int kStageCell = 2048;
+constexpr size_t stage_smem(int cap) { return sizeof(uint16_t) * kPairWarps * (size_t)cap; }
 
 struct CellDesc {
   int32_t b0, b1;  // candidate slots
@@ -185,7 +191,8 @@ __device__ __forceinline__ void div_mod_fast(int32_t v, int32_t m, int32_t& rem,
 template <bool EMIT, int K>
 __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
     k_pair_tasks(GridParams g, GridBuffers b, int64_t n, int32_t n_cells, PairBands pb,
-                 uint32_t* __restrict__ counts, const int64_t* __restrict__ offs, EmitTargets t) {
+                 uint32_t* __restrict__ counts, const int64_t* __restrict__ offs, EmitTargets t,
+                 int32_t stage_cap) {
   // Staged candidates as pairs (2m, 2m + 1): {x, x', y, y'}, {z, z'}, {idx, idx'}.
   __shared__ float4 stage_xy[kPairWarps][16];
   __shared__ float2 stage_z[kPairWarps][16];
@@ -193,11 +200,11 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
   __shared__ SlotMeta stage_m[kPairWarps][32];
   __shared__ char4 stencil[kPairMaxCells];  // (dx, dy, dz) of each stencil cell, x outer
   // Emit pass: per warp, each lane's first output slot minus its stage offset,
-  // each lane's atom meta, and the staged hits (lane << 16 | candidate offset
+  // each lane's atom meta, and the staged hits (lane << 11 | candidate offset
   // in the cell) of the current task.
   __shared__ int64_t lane_base[EMIT ? kPairWarps : 1][32];
   __shared__ SlotMeta lane_meta[EMIT ? kPairWarps : 1][32];
-  extern __shared__ uint32_t stage_hits[];
+  extern __shared__ uint16_t stage_hits[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   {
     const int32_t ny = 2 * g.ns[1] + 1, nz = 2 * g.ns[2] + 1;
@@ -279,8 +286,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
           }
           const int32_t total = __shfl_sync(0xffffffffu, pre, 31);
           pre -= cnt;
-          if (total <= kStageCap && h1 - h0 <= 65536) {
-            uint32_t* st = stage_hits + warp * kStageCap;
+          if (total <= stage_cap && h1 - h0 <= kStageCell) {
+            uint16_t* st = stage_hits + warp * stage_cap;
             lane_base[warp][lane] = slot - pre;
             lane_meta[warp][lane] = mi;
             int32_t r = pre;
@@ -290,7 +297,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
               while (hits) {
                 const int jj = __ffs(hits) - 1;
                 hits &= hits - 1;
-                if (r < r_end) st[r] = ((uint32_t)lane << 16) | (uint32_t)(jb - h0 + jj);
+                if (r < r_end) st[r] = (uint16_t)((lane << 11) | (jb - h0 + jj));
                 ++r;
               }
             }
@@ -304,13 +311,13 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
               for (int u = 0; u < 4; ++u) {
                 const int32_t k = k0 + 32 * u;
                 v[u] = k < total ? st[k] : 0u;
-                if (k < total) mj[u] = b.meta[h0 + (int32_t)(v[u] & 0xffffu)];
+                if (k < total) mj[u] = b.meta[h0 + (int32_t)(v[u] & 2047u)];
               }
 #pragma unroll
               for (int u = 0; u < 4; ++u) {
                 const int32_t k = k0 + 32 * u;
                 if (k >= total) break;
-                const int l = (int)(v[u] >> 16);
+                const int l = (int)(v[u] >> 11);
                 const SlotMeta ml = lane_meta[warp][l];
                 const int64_t e = lane_base[warp][l] + k;
                 srcq[e] = (int64_t)ml.orig + t.index_offset;
@@ -574,7 +581,8 @@ void pair_count_k(const GridParams& g, const GridBuffers& b, int64_t n, const Pa
   EmitTargets t{};
   const int32_t cells = stencil_cells(g);
   launch_pdl(k_pair_tasks<false, K>, dim3(pair_grid((const void*)k_pair_tasks<false, K>, 0)),
-             dim3(kPairWarps * 32), 0, s, g, b, n, cells, pb, counts, (const int64_t*)nullptr, t);
+             dim3(kPairWarps * 32), 0, s, g, b, n, cells, pb, counts, (const int64_t*)nullptr, t,
+             (int32_t)0);
   note_launches(1);
 }
 
@@ -582,10 +590,15 @@ template <int K>
 void pair_emit_k(const GridParams& g, const GridBuffers& b, int64_t n, const PairBands& pb,
                  const int64_t* offs, const EmitTargets& t, cudaStream_t s) {
   const int32_t cells = stencil_cells(g);
-  ensure_smem_attr((const void*)k_pair_tasks<true, K>, (int)kEmitSmem);
+  // A task's hits are at most 32 x (candidates of one cell); judge by the
+  // mean bin occupancy.
+  const double per_bin = g.total_bins > 0 ? (double)n / (double)g.total_bins : 0.0;
+  const int32_t cap = 32.0 * per_bin > (double)kStageSmall ? kStageLarge : kStageSmall;
+  ensure_smem_attr((const void*)k_pair_tasks<true, K>, (int)stage_smem(kStageLarge));
   launch_pdl(k_pair_tasks<true, K>,
-             dim3(pair_grid((const void*)k_pair_tasks<true, K>, kEmitSmem)),
-             dim3(kPairWarps * 32), kEmitSmem, s, g, b, n, cells, pb, (uint32_t*)nullptr, offs, t);
+             dim3(pair_grid((const void*)k_pair_tasks<true, K>, stage_smem(cap))),
+             dim3(kPairWarps * 32), stage_smem(cap), s, g, b, n, cells, pb, (uint32_t*)nullptr,
+             offs, t, cap);
   note_launches(1);
 }
 
