@@ -327,6 +327,18 @@ def e2e_time(nl, pos, rows, rc, steps, warmup):
     return t, m
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_oracle_time(pos, rows, rc, budget_s=4.0, min_reps=15, threads=None):
     import oracle
 
@@ -380,7 +392,8 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{args.steps} full builds of the workload (C++ restatement "
                                    "of the reference rayon count/fill path; the Rust crate "
-                                   "cannot be built here)"},
+                                   "cannot be built here)",
+                         "cpu_model": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -455,10 +468,14 @@ def run_b200(args):
     }
     if rank == 0:
         t_cpu, m_cpu, threads, reps = cpu_oracle_time(pos, rows, args.rc)
+        t_one, m_one, _, reps_one = cpu_oracle_time(pos, rows, args.rc, budget_s=1.0,
+                                                    min_reps=3, threads=1)
         line["cpu_baseline"] = {
             "value": m_cpu / t_cpu, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{reps} full builds of the workload (mean), C++ restatement of the "
-                      "reference's rayon count/fill path"}
+                      "reference's rayon count/fill path",
+            "cpu_model": cpu_model(),
+            "one_thread": {"value": m_one / t_one, "unit": UNIT, "builds": reps_one}}
         if not args.no_extra:
             line["extra"] = extra_measurements(nl, torch, args)
         print(json.dumps(line), flush=True)
