@@ -230,6 +230,15 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
   }
   const uint32_t n_tasks = (uint32_t)b.counters[0] * (uint32_t)n_cells;
   const uint32_t step = gridDim.x * kPairWarps;
+  // Emit on dense grids: tasks from a shared counter, so that warps that
+  // drew cheap tasks take more (static striding leaves a long tail there).
+  uint32_t* const queue = EMIT ? b.emit_queue : nullptr;
+  auto next_task = [&](uint32_t cur) -> uint32_t {
+    if (!queue) return cur + step;
+    uint32_t v = 0;
+    if (lane == 0) v = atomicAdd(queue, 1u);
+    return __shfl_sync(0xffffffffu, v, 0);
+  };
   int64_t off0[K];
   float lo[K], hi[K];
 #pragma unroll
@@ -239,7 +248,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
     hi[q] = pb.q[q].hi;
   }
 
-  for (uint32_t task = blockIdx.x * kPairWarps + warp; task < n_tasks; task += step) {
+  for (uint32_t task = queue ? next_task(0) : blockIdx.x * kPairWarps + warp; task < n_tasks;
+       task = next_task(task)) {
     const uint32_t gi = task / (uint32_t)n_cells;
     const int32_t c = (int32_t)(task - gi * (uint32_t)n_cells);
     const GroupRec grp = b.groups[gi];
@@ -594,10 +604,12 @@ void pair_emit_k(const GridParams& g, const GridBuffers& b, int64_t n, const Pai
   // mean bin occupancy.
   const double per_bin = g.total_bins > 0 ? (double)n / (double)g.total_bins : 0.0;
   const int32_t cap = 32.0 * per_bin > (double)kStageSmall ? kStageLarge : kStageSmall;
+  GridBuffers bq = b;
+  if (cap != kStageLarge) bq.emit_queue = nullptr;  // cheap, even tasks: static striding
   ensure_smem_attr((const void*)k_pair_tasks<true, K>, (int)stage_smem(kStageLarge));
   launch_pdl(k_pair_tasks<true, K>,
              dim3(pair_grid((const void*)k_pair_tasks<true, K>, stage_smem(cap))),
-             dim3(kPairWarps * 32), stage_smem(cap), s, g, b, n, cells, pb, (uint32_t*)nullptr,
+             dim3(kPairWarps * 32), stage_smem(cap), s, g, bq, n, cells, pb, (uint32_t*)nullptr,
              offs, t, cap);
   note_launches(1);
 }

@@ -415,11 +415,12 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
                           c.rank_nb[2] == sp.grid.nb[2];
     // One zeroed block: bin histogram, scatter cursors, pair-task counters,
     // 64-bit hit-mask cursor (8-byte aligned: 2 nb + 2 is even), build
-    // completion count.
+    // completion count, emit task counter.
     int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, 2 * (size_t)nb + 6);
     b.bin_count = zeroed;
     b.bin_fill = zeroed ? zeroed + nb : nullptr;
     b.build_done = zeroed ? zeroed + 2 * nb + 4 : nullptr;
+    b.emit_queue = zeroed ? reinterpret_cast<uint32_t*>(zeroed + 2 * nb + 5) : nullptr;
     b.bin_start = slot<int64_t>(c, kSlotBinStart, nb + 1);
     b.key = slot<uint64_t>(c, kSlotKey, n);
     b.rank = slot<int32_t>(c, kSlotRank, n);

@@ -94,7 +94,8 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
                    c.rank_nb[1] == sp.grid.nb[1] && c.rank_nb[2] == sp.grid.nb[2];
   // Zeroed block: bin histogram, scatter cursors, 2 task counters, 64-bit
   // mask cursor (8-byte aligned: 2 nb + 2 is even), build completion count,
-  // then the offsets scan's state (8-byte aligned at 2 nb + 6), so a single
+  // emit task counter, then the offsets scan's state (8-byte aligned at
+  // 2 nb + 6), so a single
   // memset at the start clears everything and the kernels follow each other
   // directly.
   sp.zeroed_words = 2 * (size_t)nb + 6 + 2 * (size_t)scan_tmp_elems(row);
@@ -105,6 +106,7 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   b.counters = zeroed ? zeroed + 2 * nb : nullptr;
   b.mask_top = zeroed ? reinterpret_cast<unsigned long long*>(zeroed + 2 * nb + 2) : nullptr;
   b.build_done = zeroed ? zeroed + 2 * nb + 4 : nullptr;
+  b.emit_queue = zeroed ? reinterpret_cast<uint32_t*>(zeroed + 2 * nb + 5) : nullptr;
   const int64_t max_tasks = (n / 32 + std::min<int64_t>(n, nb) + 1) * cells;
   b.task_hdr = slot<int4>(c, kSlotTaskHdr, max_tasks);
   b.masks = slot<uint32_t>(c, kSlotMasks, mask_cap);

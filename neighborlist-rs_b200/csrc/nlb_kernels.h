@@ -59,6 +59,10 @@ struct GridBuffers {
   // k_prep, whose last CTA then scans the bin histogram into bin_start
   // itself (grids of at most kFusedBinScanMax bins); nullptr: separate scan.
   int32_t* build_done;
+  // Optional (zeroed by the caller before the build): task counter of the
+  // pair-task emit pass, which then hands tasks out dynamically on dense
+  // grids (expensive, uneven tasks); nullptr: static assignment.
+  uint32_t* emit_queue;
   // Optional (masks == nullptr: the emit pass recomputes every test): the
   // count pass stores, per pair task, the candidate range, image shift and a
   // 32-bit hit mask per lane per 32-candidate chunk per cutoff in `masks`
