@@ -48,6 +48,12 @@ constexpr int kMaxDevices = 64;
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Scan state for the largest scans here (n + 1 counts, a bin histogram).
+constexpr int64_t kNoAllocScanWords = 64;
+static_assert((kNoAllocMaxAtoms + 1 + kScanTile - 1) / kScanTile + 2 <= kNoAllocScanWords &&
+                  (kNoAllocMaxBins + kScanTile - 1) / kScanTile + 2 <= kNoAllocScanWords,
+              "scan state of the scratch array too small for the scan tile");
+
 // Byte layout of the scratch array (each piece 256-byte aligned).
 struct Layout {
   size_t rank_of_bin, bin_count, bin_fill, bin_start, key, rank, skey, sidx, skey2, sidx2, px,
@@ -73,7 +79,7 @@ constexpr Layout make_layout() {
   L.meta = o; o += align256(sizeof(SlotMeta) * kNoAllocMaxAtoms);
   L.counts = o; o += align256(sizeof(uint32_t) * (kNoAllocMaxAtoms + 1));
   L.offs = o; o += align256(sizeof(int64_t) * (kNoAllocMaxAtoms + 2));
-  L.scan_tmp = o; o += align256(sizeof(int64_t) * 64);
+  L.scan_tmp = o; o += align256(sizeof(int64_t) * kNoAllocScanWords);
   L.bounds = o; o += align256(sizeof(double) * 6);
   L.total = o;
   return L;

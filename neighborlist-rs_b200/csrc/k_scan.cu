@@ -17,8 +17,9 @@ namespace nlb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;  // 4096 elements
+constexpr int kTile = (int)kScanTile;
+constexpr int kItems = kTile / kThreads;
+static_assert(kItems * kThreads == kTile, "tile = threads x items");
 constexpr int kPadShift = 5;              // one padding word per 32 elements
 constexpr int kSpinLimit = 1 << 22;
 

@@ -11,7 +11,8 @@ namespace nlb {
 
 // ---- k_scan.cu
 // Exclusive scan of n values into out[0..n]; out[n] = total.  `tmp` needs
-// scan_tmp_elems(n) int64 elements.
+// scan_tmp_elems(n) = ceil(n / kScanTile) + 2 int64 elements.
+constexpr int64_t kScanTile = 2048;  // elements per CTA (measured best of 1024-4096)
 int64_t scan_tmp_elems(int64_t n);
 void exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, int64_t* tmp,
                         cudaStream_t s);

@@ -316,6 +316,21 @@ def test_large_system_many_scan_tiles(nl, oracle):
         single(nl, oracle, small, eye(L * 0.5), rc, what=f"grid change rc {rc}")
 
 
+def test_million_atoms_rc8(nl, oracle):
+    """The largest served size: 1e6 atoms at rho 0.1 in a periodic box, rc 8
+    (~1.1e8 edges, 3 GB of results), every edge and shift against the oracle."""
+    import os
+
+    rng = np.random.default_rng(1_000_000)
+    L = (1_000_000 / 0.1) ** (1 / 3)
+    pos = rng.random((1_000_000, 3)) * L
+    cell = nl.PyCell(eye(L).tolist())
+    got = nl.build_neighborlists(cell, pos, 8.0)
+    ref = oracle.search_single(pos, eye(L), PBC3, 8.0, nthreads=os.cpu_count() or 8)
+    assert got["edge_index"].shape[1] > 100_000_000
+    assert_same(got, ref, "1e6 atoms rc 8")
+
+
 @pytest.mark.parametrize("rc", [6.0, 14.0])
 def test_repeated_calls_graph_replay(nl, oracle, rc):
     """Identical repeated builds: first direct, then captured, then replayed
