@@ -722,7 +722,7 @@ def served_measurements(nl):
         res["saturated_c_abi"] = run_stream_raw(srv, small)
         run_stream_raw(srv, small, device=True)
         res["saturated_c_abi_device_results"] = run_stream_raw(srv, small, device=True)
-        for rate in (2000, 10000, 25000):
+        for rate in (1000, 2000, 10000, 25000, 50000):
             k = min(len(small), max(512, int(rate * 0.4)))
             res[f"poisson_{rate}"] = run_stream(srv, small[:k], rate, seed=rate)
         st = srv.stats()
