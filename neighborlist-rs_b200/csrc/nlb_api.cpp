@@ -126,7 +126,9 @@ struct PinnedPool {
     bump_left = 0;
   }
 
-  // Takes a class-k block from the free list or the current chunk (under mu).
+  // Takes a class-k block from the free list, the current chunk, or by
+  // splitting the smallest larger free block in halves (under mu); only when
+  // all three fail does the caller pin a new chunk.
   void* take_class_locked(int k) {
     if (!free_class[k].empty()) {
       void* p = free_class[k].back();
@@ -139,6 +141,14 @@ struct PinnedPool {
       void* p = bump;
       bump += b;
       bump_left -= b;
+      return p;
+    }
+    for (int j = k + 1; j <= kMaxShift; ++j) {
+      if (free_class[j].empty()) continue;
+      char* p = static_cast<char*>(free_class[j].back());
+      free_class[j].pop_back();
+      for (int i = j - 1; i >= k; --i) free_class[i].push_back(p + (size_t(1) << i));
+      ++n_hits;
       return p;
     }
     return nullptr;
