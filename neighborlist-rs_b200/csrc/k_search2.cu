@@ -259,6 +259,18 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
     if (EMIT && b.masks) {
       // Hits recorded by the count pass: expand the stored masks.
       const int4 hdr = b.task_hdr[task];
+      // Loads that need no header, issued before its branch so that their
+      // latency overlaps the header's.
+      SlotMeta mi{};
+      int64_t o_lo = 0, o_hi = 0;
+      if (lane < len) {
+        mi = b.meta[p];
+        if (K == 1) {
+          const int64_t idx = (int64_t)p * n_cells + c;
+          o_lo = offs[idx];
+          o_hi = offs[idx + 1];
+        }
+      }
       if (hdr.x == -2) continue;
       if (hdr.x >= 0) {
         const int32_t h0 = hdr.y, h1 = hdr.z;
@@ -267,8 +279,6 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
         const int32_t s0 = (int32_t)(pw << 22) >> 22;
         const int32_t s1 = (int32_t)(pw << 12) >> 22;
         const int32_t s2 = (int32_t)(pw << 2) >> 22;
-        SlotMeta mi{};
-        if (mine) mi = b.meta[p];
 #pragma unroll 1
         for (int q = 0; q < K; ++q) {
           int64_t* __restrict__ srcq = t.src[q];
@@ -277,7 +287,10 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
           const uint32_t* mq = b.masks + (int64_t)hdr.x + (int64_t)q * words;
           int64_t slot = 0;
           int32_t cnt = 0;
-          if (mine) {
+          if (mine && K == 1) {
+            slot = t.base[0] + (o_lo - off0[0]);
+            cnt = (int32_t)(o_hi - o_lo);
+          } else if (mine) {
             const int64_t idx = q * pb.row + (int64_t)p * n_cells + c;
             const int64_t o0 = offs[idx];
             slot = t.base[q] + (o0 - off0[q]);
