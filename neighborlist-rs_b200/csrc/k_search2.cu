@@ -184,12 +184,11 @@ __device__ __forceinline__ void div_mod_fast(int32_t v, int32_t m, int32_t& rem,
   }
 }
 
-// Register budgets measured best on B200: the single-cutoff count pass at 3
-// CTAs per SM (2 with several cutoffs, which need more masks live); the emit
-// pass unbounded (120 registers, 2 CTAs per SM), which beats a spilling
-// 80-register build.
+// Register budgets measured best on B200: the single-cutoff passes at 3 CTAs
+// per SM (80 registers, no spills); with several cutoffs, which keep more
+// masks live, the count pass at 2 and the emit pass unbounded.
 template <bool EMIT, int K>
-__global__ void __launch_bounds__(kPairWarps * 32, EMIT ? 1 : (K == 1 ? 3 : 2))
+__global__ void __launch_bounds__(kPairWarps * 32, EMIT ? (K == 1 ? 3 : 1) : (K == 1 ? 3 : 2))
     k_pair_tasks(GridParams g, GridBuffers b, int64_t n, int32_t n_cells, PairBands pb,
                  uint32_t* __restrict__ counts, const int64_t* __restrict__ offs, EmitTargets t,
                  int32_t stage_cap) {
