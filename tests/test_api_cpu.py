@@ -156,3 +156,38 @@ def test_threads_and_logging(nl):
     assert nl.get_num_threads() > 0
     nl.init_logging("debug")
     nl.init_logging(None)
+
+
+def test_batch_launch_shapes_and_pinning(nl):
+    """The batched kernels' launch-shape table and the pin / reset calls are
+    host-side: every shape is a valid launch, pinning checks its range."""
+    n = nl.set_batch_shape(None)
+    assert n >= 2
+    seen = set()
+    for i in range(n):
+        s = nl.batch_shape_info(i)
+        assert s["small_threads"] in (64, 128, 256, 512)
+        assert s["large_threads"] in (256, 512)
+        assert s["chunk"] in (128, 256, 512) and s["large_atoms"] >= 256
+        seen.add(tuple(s.values()))
+    assert len(seen) == n, "duplicate shapes"
+    assert nl.batch_shape_info(0) == {"small_threads": 256, "large_threads": 512, "chunk": 256,
+                                      "large_atoms": 512}
+    try:
+        assert nl.set_batch_shape(n - 1) == n
+    finally:
+        nl.set_batch_shape(None)
+    for bad in (n, -2):
+        with pytest.raises(ValueError):
+            nl.set_batch_shape(bad)
+        with pytest.raises(ValueError):
+            nl.batch_shape_info(bad)
+    nl.batch_tuner_reset()
+    assert nl.batch_tuner_state() == []
+
+
+def test_pinned_stats_counters(nl):
+    st = nl.pinned_stats()
+    assert set(st) == {"host_alloc_calls", "host_alloc_us", "host_alloc_bytes", "host_free_calls",
+                       "host_free_us", "cache_hits", "cached_bytes"}
+    assert all(isinstance(v, int) and v >= 0 for v in st.values())
