@@ -79,6 +79,20 @@ int nlb_build_batch_multi(const double* positions, int64_t n_atoms, const int32_
                           const double* cells, const uint8_t* pbcs, const uint8_t* has_cell,
                           int64_t n_cells, int disjoint, nlb_result* outs);
 
+/* The batched build with a per-system offset table on the output (no
+ * counterpart in the reference, whose batched result is the concatenated
+ * list only).  Arguments as nlb_build_batch_multi; multi = 0 gives the
+ * single-cutoff semantics of nlb_build_batch (n_cutoffs = 1).  When
+ * system_offsets is not NULL it receives n_cutoffs rows of n_systems + 1
+ * int64 (row = input cutoff index; n_systems counts the batch-id runs, 0 for
+ * an empty input): system i's edges of that list are [row[i], row[i + 1]).
+ * The table comes from the device's count pass at no extra synchronisation. */
+int nlb_build_batch_ex(const double* positions, int64_t n_atoms, const int32_t* batch,
+                       int64_t n_batch, const double* cutoffs, int32_t n_cutoffs,
+                       const double* cells, const uint8_t* pbcs, const uint8_t* has_cell,
+                       int64_t n_cells, int disjoint, int multi, nlb_result* outs,
+                       int64_t* system_offsets);
+
 /* Releases both arrays of a result (safe on a zeroed struct). */
 void nlb_result_free(nlb_result* r);
 /* Releases one array obtained from a result (for callers that hand the two

@@ -1034,6 +1034,17 @@ int nlb_build_batch_multi(const double* positions, int64_t n_atoms, const int32_
       .code;
 }
 
+int nlb_build_batch_ex(const double* positions, int64_t n_atoms, const int32_t* batch,
+                       int64_t n_batch, const double* cutoffs, int32_t n_cutoffs,
+                       const double* cells, const uint8_t* pbcs, const uint8_t* has_cell,
+                       int64_t n_cells, int disjoint, int multi, nlb_result* outs,
+                       int64_t* system_offsets) {
+  if (n_cutoffs > 0 && (!outs || !cutoffs)) return fail(NLB_ERR_VALUE, "outs is NULL").code;
+  return run_batch(positions, n_atoms, batch, n_batch, cutoffs, n_cutoffs, cells, pbcs, has_cell,
+                   n_cells, disjoint != 0, multi != 0, outs, system_offsets)
+      .code;
+}
+
 int nlb_build_ex(const double* positions, int64_t n_atoms, double cutoff, const double* cell,
                  const uint8_t* pbc, int flags, nlb_result_ex* out) {
   if (!out) return fail(NLB_ERR_VALUE, "out is NULL").code;

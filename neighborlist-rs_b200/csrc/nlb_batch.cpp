@@ -80,10 +80,13 @@ CutoffSet make_pass(const std::vector<double>& rc_sq, int32_t g0, bool disjoint)
 }
 
 // One run [a, b) of small systems through the batched kernels.
+// With sys_off (k rows of n_systems + 1, sorted cutoff order), also writes
+// the first edge of each of systems [a, b) in every list.
 Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts,
                  const int64_t* d_starts, const double* d_cells, const uint8_t* d_pbcs,
                  const uint8_t* d_has, int32_t a, int32_t b, double rc_max,
-                 const std::vector<double>& rc_sq, bool disjoint, bool multi, Outputs& out) {
+                 const std::vector<double>& rc_sq, bool disjoint, bool multi, Outputs& out,
+                 std::vector<int64_t>* sys_off) {
   cudaStream_t s = c.stream;
   const int32_t ns = b - a;
   const int32_t k = (int32_t)rc_sq.size();
@@ -129,6 +132,17 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
   c.mark(2);
   exclusive_scan_u32(counts, (int64_t)k * row, offs, scan_tmp, s);
   c.mark(3);
+  // Per-system edge offsets within this run, one row of ns + 1 per cutoff.
+  std::vector<int64_t> run_bounds;
+  if (sys_off) {
+    int64_t* d_bounds = slot<int64_t>(c, kSlotBatch0 + 11, (size_t)k * (ns + 1));
+    if (!d_bounds) return fail(NLB_ERR_NOMEM, "device allocation failed");
+    for (int32_t q = 0; q < k; ++q)
+      launch_sys_bounds(plans, ns, offs + (size_t)q * row, row, d_bounds + (size_t)q * (ns + 1), s);
+    run_bounds.resize((size_t)k * (ns + 1));
+    cudaMemcpyAsync(run_bounds.data(), d_bounds, sizeof(int64_t) * run_bounds.size(),
+                    cudaMemcpyDeviceToHost, s);
+  }
   if (k + 3 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
   cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), offs, sizeof(int64_t) * row,
                                     sizeof(int64_t), (size_t)k + 1, cudaMemcpyDeviceToHost, s);
@@ -150,6 +164,12 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
   if (plan_err == 2) return fail(NLB_ERR_VALUE, "stencil too large for this cutoff and cell");
   std::vector<int64_t> m(k);
   for (int32_t q = 0; q < k; ++q) m[q] = c.h_small[q + 1] - c.h_small[q];
+  if (sys_off) {
+    const size_t stride = starts.size();  // n_systems + 1
+    for (int32_t q = 0; q < k; ++q)
+      for (int32_t i = 0; i < ns; ++i)
+        (*sys_off)[(size_t)q * stride + a + i] = out.total[q] + run_bounds[(size_t)q * (ns + 1) + i];
+  }
   if (!out.reserve(m, s)) return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
 
   const BatchItems& bw = trials.pick(c);
@@ -180,14 +200,17 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
 Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_batch,
                  const double* cutoffs, int32_t k, const double* cells, const uint8_t* pbcs,
                  const uint8_t* has_cell, int64_t n_cells, bool disjoint, bool multi,
-                 nlb_result* outs) {
+                 nlb_result* outs, int64_t* sys_offsets) {
   zero_results(outs, k);
   if (n_batch != n) return fail(NLB_ERR_VALUE, "positions and batch must have the same length");
   if (k <= 0) return Status{NLB_OK};
   if (!cutoffs_valid(cutoffs, k))
     return fail(NLB_ERR_VALUE, multi ? "All cutoffs must be positive and finite"
                                      : "Cutoff must be positive and finite");
-  if (n == 0) return empty_results(outs, k);
+  if (n == 0) {
+    if (sys_offsets) std::memset(sys_offsets, 0, sizeof(int64_t) * (size_t)k);  // no systems
+    return empty_results(outs, k);
+  }
   if (!pos || !batch) return fail(NLB_ERR_VALUE, "positions or batch is NULL");
 
   std::vector<int64_t> starts;
@@ -239,6 +262,9 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
   }
 
   Outputs out(*c, k);
+  // Per-system offsets in sorted cutoff order while the runs go by.
+  std::vector<int64_t> sys_off;
+  if (sys_offsets) sys_off.assign((size_t)k * starts.size(), 0);
   int32_t i = 0;
   while (i < n_sys) {
     const int64_t ni = starts[i + 1] - starts[i];
@@ -246,7 +272,7 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
       int32_t j = i;
       while (j < n_sys && starts[j + 1] - starts[j] <= kBatchMaxAtoms) ++j;
       st = run_small(*c, d_pos, starts, d_starts, d_cells, d_pbcs, d_has, i, j, rc_max, rc_sq,
-                     disjoint, multi, out);
+                     disjoint, multi, out, sys_offsets ? &sys_off : nullptr);
       if (!st.ok()) return st;
       i = j;
       continue;
@@ -275,7 +301,10 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
     }
     st = emit_system(*c, sp, d_pos + 3 * starts[i], L, out.total.data(), starts[i]);
     if (!st.ok()) return st;
-    for (int32_t q = 0; q < k; ++q) out.total[q] += sp.m[q];
+    for (int32_t q = 0; q < k; ++q) {
+      if (sys_offsets) sys_off[(size_t)q * starts.size() + i] = out.total[q];
+      out.total[q] += sp.m[q];
+    }
     ++i;
   }
 
@@ -288,6 +317,14 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
     cudaMemcpyAsync(r.edge_index, out.src(q), 8 * m, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(r.edge_index + m, out.dst(q), 8 * m, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(r.shift, out.shf(q), 12 * m, cudaMemcpyDeviceToHost, s);
+  }
+  if (sys_offsets) {
+    const size_t stride = starts.size();
+    for (int32_t q = 0; q < k; ++q) {
+      sys_off[(size_t)q * stride + n_sys] = out.total[q];
+      std::memcpy(sys_offsets + (size_t)order[q] * stride, sys_off.data() + (size_t)q * stride,
+                  sizeof(int64_t) * stride);
+    }
   }
   cudaError_t e = cudaStreamSynchronize(s);
   if (c->prof) c->harvest();

@@ -203,9 +203,11 @@ struct ShapeTrials {
 };
 void tune_release(Ctx& c);
 
+// sys_offsets (optional): k x (n_systems + 1) int64, row = input cutoff
+// index; system i's edges of that list are [row[i], row[i + 1]).
 Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_batch,
                  const double* cutoffs, int32_t k, const double* cells, const uint8_t* pbcs,
                  const uint8_t* has_cell, int64_t n_cells, bool disjoint, bool multi,
-                 nlb_result* outs);
+                 nlb_result* outs, int64_t* sys_offsets = nullptr);
 
 }  // namespace nlb

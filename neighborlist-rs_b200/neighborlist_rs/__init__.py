@@ -59,6 +59,10 @@ _lib.nlb_build_batch.argtypes = [_dp, ctypes.c_int64, _i32p, ctypes.c_int64, cty
 _lib.nlb_build_batch_multi.argtypes = [_dp, ctypes.c_int64, _i32p, ctypes.c_int64, _dp,
                                        ctypes.c_int32, _dp, _u8p, _u8p, ctypes.c_int64,
                                        ctypes.c_int, ctypes.POINTER(_Result)]
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_lib.nlb_build_batch_ex.argtypes = [_dp, ctypes.c_int64, _i32p, ctypes.c_int64, _dp,
+                                    ctypes.c_int32, _dp, _u8p, _u8p, ctypes.c_int64,
+                                    ctypes.c_int, ctypes.c_int, ctypes.POINTER(_Result), _i64p]
 _lib.nlb_result_free.argtypes = [ctypes.POINTER(_Result)]
 _lib.nlb_host_free.argtypes = [ctypes.c_void_p]
 _lib.nlb_cell_check.argtypes = [_dp]
@@ -306,9 +310,13 @@ def _batch_cells(cells, batch):
     return n_sys, h9, pbcs, has, n_sys
 
 
-def build_neighborlists_batch(positions, batch, cells=None, cutoff=5.0, parallel=True):
+def build_neighborlists_batch(positions, batch, cells=None, cutoff=5.0, parallel=True, *,
+                              return_offsets=False):
     """src/python_api.rs:315-423.  Systems split wherever the batch id
-    changes; indices are global; systems concatenated in order."""
+    changes; indices are global; systems concatenated in order.
+
+    ``return_offsets=True`` (an addition) also returns ``system_offsets``,
+    int64 (n_systems + 1,): system i's edges are [off[i], off[i + 1])."""
     c = _check_cutoff(cutoff)
     pos = _positions(positions)
     b = _batch_ids(batch)
@@ -316,21 +324,33 @@ def build_neighborlists_batch(positions, batch, cells=None, cutoff=5.0, parallel
     if b.shape[0] != n:
         raise ValueError("positions and batch must have the same length")
     if n == 0:
-        return _empty()
-    _, h9, pbcs, has, nc = _batch_cells(cells, b)
+        res = _empty()
+        if return_offsets:
+            res["system_offsets"] = np.zeros(1, np.int64)
+        return res
+    n_sys, h9, pbcs, has, nc = _batch_cells(cells, b)
     r = _Result()
-    _check(_lib.nlb_build_batch(
-        pos.ctypes.data_as(_dp), n, b.ctypes.data_as(_i32p), n, c,
-        h9.ctypes.data_as(_dp) if h9 is not None else None,
-        pbcs.ctypes.data_as(_u8p) if pbcs is not None else None,
-        has.ctypes.data_as(_u8p) if has is not None else None, nc, int(bool(parallel)),
-        ctypes.byref(r)))
-    return _to_dict(r)
+    cells_args = (h9.ctypes.data_as(_dp) if h9 is not None else None,
+                  pbcs.ctypes.data_as(_u8p) if pbcs is not None else None,
+                  has.ctypes.data_as(_u8p) if has is not None else None, nc)
+    if not return_offsets:
+        _check(_lib.nlb_build_batch(pos.ctypes.data_as(_dp), n, b.ctypes.data_as(_i32p), n, c,
+                                    *cells_args, int(bool(parallel)), ctypes.byref(r)))
+        return _to_dict(r)
+    carr = np.array([c], dtype=np.float64)
+    offs = np.zeros(n_sys + 1, np.int64)
+    _check(_lib.nlb_build_batch_ex(pos.ctypes.data_as(_dp), n, b.ctypes.data_as(_i32p), n,
+                                   carr.ctypes.data_as(_dp), 1, *cells_args, 0, 0,
+                                   ctypes.byref(r), offs.ctypes.data_as(_i64p)))
+    res = _to_dict(r)
+    res["system_offsets"] = offs
+    return res
 
 
 def build_neighborlists_batch_multi(positions, batch, cells=None, cutoffs=(5.0,), labels=None,
-                                    disjoint=False):
-    """src/python_api.rs:425-546."""
+                                    disjoint=False, *, return_offsets=False):
+    """src/python_api.rs:425-546.  ``return_offsets=True`` (an addition) adds
+    ``system_offsets`` to each list, as in build_neighborlists_batch."""
     pos = _positions(positions)
     b = _batch_ids(batch)
     n = pos.shape[0]
@@ -345,16 +365,28 @@ def build_neighborlists_batch_multi(positions, batch, cells=None, cutoffs=(5.0,)
         labels = [str(x) for x in labels]
         if len(labels) != len(cs):
             raise ValueError("Length of labels must match length of cutoffs")
-    _, h9, pbcs, has, nc = _batch_cells(cells, b)
+    n_sys, h9, pbcs, has, nc = _batch_cells(cells, b)
     k = len(cs)
     carr = np.ascontiguousarray(np.array(cs, dtype=np.float64))
     outs = (_Result * k)()
-    _check(_lib.nlb_build_batch_multi(
+    cells_args = (h9.ctypes.data_as(_dp) if h9 is not None else None,
+                  pbcs.ctypes.data_as(_u8p) if pbcs is not None else None,
+                  has.ctypes.data_as(_u8p) if has is not None else None, nc)
+    if not return_offsets:
+        _check(_lib.nlb_build_batch_multi(
+            pos.ctypes.data_as(_dp), n, b.ctypes.data_as(_i32p), n, carr.ctypes.data_as(_dp), k,
+            *cells_args, int(bool(disjoint)), outs))
+        return _multi_dict([_to_dict(outs[q]) for q in range(k)], labels)
+    offs = np.zeros((k, n_sys + 1), np.int64)
+    _check(_lib.nlb_build_batch_ex(
         pos.ctypes.data_as(_dp), n, b.ctypes.data_as(_i32p), n, carr.ctypes.data_as(_dp), k,
-        h9.ctypes.data_as(_dp) if h9 is not None else None,
-        pbcs.ctypes.data_as(_u8p) if pbcs is not None else None,
-        has.ctypes.data_as(_u8p) if has is not None else None, nc, int(bool(disjoint)), outs))
-    return _multi_dict([_to_dict(outs[q]) for q in range(k)], labels)
+        *cells_args, int(bool(disjoint)), 1, outs, offs.ctypes.data_as(_i64p)))
+    lists = []
+    for q in range(k):
+        d = _to_dict(outs[q])
+        d["system_offsets"] = offs[q]
+        lists.append(d)
+    return _multi_dict(lists, labels)
 
 
 # ---------------------------------------------------------------- configuration

@@ -254,6 +254,47 @@ def test_batch_mixed_sizes_and_many_cutoffs(nl, oracle):
             assert_same(gm[q], rm[q], f"batch 35 cutoffs disjoint={dj} q={q}")
 
 
+def test_batch_system_offsets(nl):
+    """The per-system offset table of a batched call: system i's edges are
+    [off[i], off[i + 1]) in every list, for systems on the batched kernels and
+    on the single-system pipeline alike; the edges are unchanged."""
+    from neighborlist_rs import workloads as W
+
+    small = W.uneven_batch(n_systems=40, seed=43)
+    rng = np.random.default_rng(44)
+    big_rows = np.diag([26.0, 26.0, 26.0])
+    big = W.System(rng.random((3000, 3)) @ big_rows, big_rows, 5.0)
+    systems = small[:15] + [big] + small[15:]
+    pos, batch, cells = W.concat_batch(systems)
+    n_sys = len(systems)
+    starts = np.concatenate([[0], np.cumsum([len(s.positions) for s in systems])])
+
+    def check(res, what):
+        off = res["system_offsets"]
+        src = res["edge_index"][0]
+        assert off.dtype == np.int64 and off.shape == (n_sys + 1,), what
+        sys_of_edge = np.searchsorted(starts, src, side="right") - 1
+        want = np.concatenate([[0], np.cumsum(np.bincount(sys_of_edge, minlength=n_sys))])
+        assert np.array_equal(off, want), what
+        assert np.all(np.diff(sys_of_edge) >= 0), what
+
+    plain = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=5.0)
+    got = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=5.0, return_offsets=True)
+    assert_same(got, (plain["edge_index"], plain["shift"]), "edges with offsets")
+    check(got, "single cutoff")
+    cs = [5.0, 3.0, 4.0]
+    for dj in (False, True):
+        pm = nl.build_neighborlists_batch_multi(pos, batch, cells=cells, cutoffs=cs, disjoint=dj)
+        gm = nl.build_neighborlists_batch_multi(pos, batch, cells=cells, cutoffs=cs, disjoint=dj,
+                                                return_offsets=True)
+        for q in range(len(cs)):
+            assert_same(gm[q], (pm[q]["edge_index"], pm[q]["shift"]), f"multi q={q} dj={dj}")
+            check(gm[q], f"multi q={q} disjoint={dj}")
+    empty = nl.build_neighborlists_batch(np.zeros((0, 3)), np.zeros(0, np.int32), cutoff=5.0,
+                                         return_offsets=True)
+    assert np.array_equal(empty["system_offsets"], [0])
+
+
 def test_batch_singular_cell(nl):
     pos = np.random.default_rng(1).random((6, 3))
     batch = np.array([0, 0, 0, 1, 1, 1], np.int32)
