@@ -191,3 +191,28 @@ def test_pinned_stats_counters(nl):
     assert set(st) == {"host_alloc_calls", "host_alloc_us", "host_alloc_bytes", "host_free_calls",
                        "host_free_us", "cache_hits", "cached_bytes"}
     assert all(isinstance(v, int) and v >= 0 for v in st.values())
+
+
+@pytest.mark.parametrize("offsets", [False, True])
+def test_batch_validation_with_and_without_offsets(nl, offsets):
+    """The batched calls raise the reference's errors before any device work
+    (src/python_api.rs:315-423, src/batch.rs:18-46), with or without the
+    per-system offset table."""
+    pos = np.zeros((4, 3))
+    with pytest.raises(ValueError, match="positions and batch must have the same length"):
+        nl.build_neighborlists_batch(pos, np.zeros(3, np.int32), cutoff=5.0,
+                                     return_offsets=offsets)
+    with pytest.raises(ValueError, match="Batch IDs must be monotonic"):
+        nl.build_neighborlists_batch(pos, np.array([0, 1, 0, 1], np.int32), cutoff=5.0,
+                                     return_offsets=offsets)
+    with pytest.raises(ValueError, match="Expected at least 2 cells, but got 1"):
+        nl.build_neighborlists_batch(pos, np.array([0, 0, 1, 1], np.int32),
+                                     cells=np.zeros((1, 3, 3)), cutoff=5.0,
+                                     return_offsets=offsets)
+    with pytest.raises(ValueError, match="All cutoffs must be positive and finite"):
+        nl.build_neighborlists_batch_multi(pos, np.zeros(4, np.int32), cutoffs=[5.0, -1.0],
+                                           return_offsets=offsets)
+    r = nl.build_neighborlists_batch(np.zeros((0, 3)), np.zeros(0, np.int32), cutoff=5.0,
+                                     return_offsets=offsets)
+    assert r["edge_index"].shape == (2, 0)
+    assert ("system_offsets" in r) == offsets
