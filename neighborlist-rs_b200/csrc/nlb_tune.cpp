@@ -23,7 +23,6 @@
 // launch, so no candidate pays for loading a module.  NLB_BATCH_SHAPE=i in
 // the environment, or nlb_batch_shape(i), pins shape i for every batch.
 #include <algorithm>
-#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <map>
@@ -63,7 +62,10 @@ void set_candidates(int64_t max_atoms, TuneEntry& e) {
   if (e.n_cand == 1) e.best = e.cand[0];
 }
 
-std::atomic<bool> g_preloaded[16];
+// Devices whose kernel variants are loaded (under g_preload_mu, so that no
+// thread times a candidate while another is still loading them).
+std::mutex g_preload_mu;
+bool g_preloaded[16] = {};
 
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;
@@ -134,8 +136,13 @@ Status ShapeTrials::prepare(Ctx& c, const TuneKey& k, const int64_t* sizes, int3
   }
   timed = shapes.size() > 1;
   if (timed) {
-    if (c.device >= 0 && c.device < 16 && !g_preloaded[c.device].exchange(true))
-      preload_batch_kernels();
+    if (c.device >= 0 && c.device < 16) {
+      std::lock_guard<std::mutex> lk(g_preload_mu);
+      if (!g_preloaded[c.device]) {
+        preload_batch_kernels();
+        g_preloaded[c.device] = true;
+      }
+    }
     for (cudaEvent_t& ev : c.tune_ev)
       if (!ev && cudaEventCreate(&ev) != cudaSuccess) {
         cudaGetLastError();
