@@ -612,7 +612,7 @@ template <int K>
 void pair_emit_k(const GridParams& g, const GridBuffers& b, int64_t n, const PairBands& pb,
                  const int64_t* offs, const EmitTargets& t, cudaStream_t s) {
   const int32_t cells = stencil_cells(g);
-  // A task's hits are at most 32 x (candidates of one cell); judge by the
+  // A task's hits are at most 32 x (candidates of one cell); decide by the
   // mean bin occupancy.
   const double per_bin = g.total_bins > 0 ? (double)n / (double)g.total_bins : 0.0;
   const int32_t cap = 32.0 * per_bin > (double)kStageSmall ? kStageLarge : kStageSmall;
