@@ -84,7 +84,7 @@ struct PinnedPool {
   std::multimap<size_t, void*> free_blocks;  // size -> block
   std::unordered_map<void*, size_t> sizes;   // every dedicated block
   size_t cached = 0;
-  static constexpr size_t kMaxCached = size_t(8) << 30;
+  static constexpr size_t kMaxCached = size_t(16) << 30;
   // Counters (nlb_pinned_stats).
   int64_t n_host_alloc = 0, us_host_alloc = 0, bytes_host_alloc = 0;
   int64_t n_host_free = 0, us_host_free = 0, n_hits = 0;
