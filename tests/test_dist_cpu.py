@@ -61,3 +61,4 @@ def test_reference_arm_prints_once_on_rank0():
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
     assert line["config"]["edges_per_step"] == 490514
+    assert line["cpu_baseline"]["cores"] >= 1 and line["cpu_baseline"]["cpu_model"]
