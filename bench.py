@@ -93,7 +93,7 @@ def settle_batch_tuner(nl, fn, limit=64):
 
 
 def _case_batch(nl, torch, steps, warmup):
-    from neighborlist_rs import workloads as W
+    W = workloads()
 
     pb, bb, cb = W.concat_batch(W.uneven_batch())
     settle_batch_tuner(nl, lambda: nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0))
@@ -106,7 +106,7 @@ def _case_batch(nl, torch, steps, warmup):
 
 
 def _case_served(nl, torch, steps, warmup):
-    from neighborlist_rs import workloads as W
+    W = workloads()
     from neighborlist_rs.serving import Server
 
     reqs = [(None if s.cell_rows is None else nl.PyCell(s.cell_rows.T.tolist()), s.positions,
@@ -120,7 +120,7 @@ def _case_served(nl, torch, steps, warmup):
 
 
 def _case_multi(nl, torch, steps, warmup):
-    from neighborlist_rs import workloads as W
+    W = workloads()
 
     p3, r3 = W.triclinic_uniform()
     cell = nl.PyCell(r3.T.tolist())
@@ -243,8 +243,28 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- workloads
 
+_WORKLOADS = None
+
+
+def workloads():
+    """The seeded workload generators (neighborlist_rs/workloads.py), loaded
+    from their file so that the CPU reference arm never imports the
+    neighborlist_rs package (whose import maps the CUDA library)."""
+    global _WORKLOADS
+    if _WORKLOADS is None:
+        import importlib.util
+
+        path = os.path.join(PKG_DIR, "neighborlist_rs", "workloads.py")
+        spec = importlib.util.spec_from_file_location("nlb_bench_workloads", path)
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[spec.name] = mod  # dataclasses resolve their module by name
+        spec.loader.exec_module(mod)
+        _WORKLOADS = mod
+    return _WORKLOADS
+
+
 def headline_system():
-    from neighborlist_rs import workloads as W
+    W = workloads()
 
     pos, rows = W.cluster_liquid()
     return pos, rows
@@ -362,6 +382,12 @@ def cpu_oracle_time(pos, rows, rc, budget_s=4.0, min_reps=15, threads=None):
 
 # ---------------------------------------------------------------- arms
 
+def bench_config(workload, atoms, edges_per_step):
+    """The `config` dict both arms print (identical for the same workload)."""
+    return {"workload": workload, "atoms": atoms, "edges_per_step": edges_per_step,
+            "l2": "flushed between steps (256 MB write)"}
+
+
 def run_reference(args):
     rank, _, world = dist_init("gloo")
     if rank != 0:
@@ -373,9 +399,13 @@ def run_reference(args):
     h, pbc = rows.T, [True] * 3
     for _ in range(args.warmup):
         oracle.search_single(pos, h, pbc, args.rc, nthreads=threads)
+    # Host caches are flushed between steps like the GPU arm's L2: a 256 MB
+    # write outside the timed spans.
+    flush = np.empty(256 << 20, np.uint8)
     t = 0.0
     m = 0
     for _ in range(args.steps):
+        flush.fill(1)
         t0 = time.perf_counter()
         ei, _ = oracle.search_single(pos, h, pbc, args.rc, nthreads=threads)
         t += time.perf_counter() - t0
@@ -389,8 +419,9 @@ def run_reference(args):
         "impl": "reference", "metric": metric, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": workload, "edges_per_step": m, "parallelism": "host threads"},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded cluster liquid)",
+        "config": bench_config(workload, int(pos.shape[0]), m),
+        "parallelism": f"{threads} host threads (rank 0 only)",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{args.steps} full builds of the workload (C++ restatement "
                                    "of the reference rayon count/fill path; the Rust crate "
@@ -457,9 +488,8 @@ def run_b200(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded cluster liquid)",
-        "config": {"workload": workload, "atoms": n, "edges_per_step": m_step,
-                   "parallelism": f"replicas x{world} (independent systems)",
-                   "l2": "flushed between steps (256 MB write)"},
+        "config": bench_config(workload, n, m_step),
+        "parallelism": f"replicas x{world} (independent systems)",
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak,
@@ -509,7 +539,7 @@ def median_call(fn, reps=5, warmup=2):
 
 
 def extra_measurements(nl, torch, args):
-    from neighborlist_rs import workloads as W
+    W = workloads()
 
     out = {}
     steps = max(5, args.steps // 3)
@@ -705,7 +735,7 @@ def served_measurements(nl):
     mix and a bounded sample of the full request-size distribution, each
     against the plain per-request loop (build_neighborlists) over the same
     requests.  Every arm runs once untimed over the same requests first."""
-    from neighborlist_rs import workloads as W
+    W = workloads()
     from neighborlist_rs.serving import Server
 
     def as_reqs(stream):

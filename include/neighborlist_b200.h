@@ -248,10 +248,12 @@ void nlb_verlet_destroy(nlb_verlet* v);
  * systems are limited to 16384 atoms and 16384 cell-list bins; larger inputs
  * and M > max_edges are rejected with NLB_ERR_VALUE (outputs untouched when
  * M > max_edges; *n_edges still reports M).  The first call on each device
- * looks up the array's device address (make it before any stream capture).
- * Calls share the array: calls that overlap on one device race and must be
- * serialised.  Runs on `stream` (a cudaStream_t, NULL = legacy default) and
- * returns after the results are complete. */
+ * looks up the array's device address (make it before any stream capture);
+ * after a cudaDeviceReset of that device, do not call it again in the same
+ * process.  Calls share the array: calls that overlap on one device race and
+ * must be serialised.  Runs on `stream` (a cudaStream_t, NULL = legacy
+ * default), synchronises that stream twice (after the count pass and after
+ * the emit pass) and returns after the results are complete. */
 int nlb_build_noalloc(const double* d_positions, int64_t n_atoms, double cutoff,
                       const double* cell, const uint8_t* pbc, int64_t* d_edge_index,
                       int32_t* d_shift, int64_t max_edges, int64_t* n_edges, void* stream);

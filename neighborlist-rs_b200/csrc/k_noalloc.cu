@@ -23,7 +23,10 @@
 // (it is a host-side stand-in), so the first call on each device, with that
 // device current, asks the runtime for the address with cudaGetSymbolAddress
 // and caches it.  That first call should therefore happen before any stream
-// capture begins.
+// capture begins.  The cached address belongs to the device's current
+// context: after a cudaDeviceReset of that device the process must not call
+// this entry point again.  Each call synchronises its stream (after the count
+// pass and after the emit pass) before it returns.
 //
 // All calls share the one array: calls that overlap on the GPU (two host
 // threads, or two streams, at once on the same device) race on it and must be
@@ -150,7 +153,8 @@ Status run_noalloc(const double* d_pos, int64_t n, double cutoff, const double* 
     double* d_b = at<double>(base, kLayout.bounds);
     double hb[6];
     launch_bounds(d_pos, n, d_b, s);
-    cudaError_t e = cudaMemcpyAsync(hb, d_b, sizeof(hb), cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hb, d_b, sizeof(hb), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(e, "bounds");
     if (!auto_box_from_bounds(hb, hb + 3, cutoff, cell, err)) return fail(NLB_ERR_VALUE, err);
@@ -161,10 +165,15 @@ Status run_noalloc(const double* d_pos, int64_t n, double cutoff, const double* 
   GridBuffers b{};
   if (method == Method::kCellList) {
     plan_grid(cell, cutoff, g);
+    // Every size check happens here, before anything is launched into the
+    // fixed scratch array.
+    for (int a = 0; a < 3; ++a)
+      if (g.nb[a] < 1 || g.nb[a] >= (1 << 21))
+        return fail(NLB_ERR_VALUE, "cell list needs more than 2^21 bins along one axis");
     for (int a = 0; a < 3; ++a)
       if (g.ns[a] < 0 || g.ns[a] > (1 << 20))
         return fail(NLB_ERR_VALUE, "stencil too large for this cutoff and cell");
-    if (g.total_bins > kNoAllocMaxBins)
+    if (g.total_bins < 1 || g.total_bins > kNoAllocMaxBins)
       return fail(NLB_ERR_VALUE, "nlb_build_noalloc: " + std::to_string(g.total_bins) +
                                      " cell-list bins exceed its fixed capacity of " +
                                      std::to_string(kNoAllocMaxBins));
@@ -200,19 +209,30 @@ Status run_noalloc(const double* d_pos, int64_t n, double cutoff, const double* 
   int64_t* scan_tmp = at<int64_t>(base, kLayout.scan_tmp);
 
   // ---- count pass (scratch re-zeroed where it must start at zero)
+  cudaError_t e = cudaSuccess;
   if (method == Method::kCellList) {
-    cudaMemsetAsync(b.bin_count, 0, sizeof(int32_t) * g.total_bins, s);
-    cudaMemsetAsync(b.bin_fill, 0, sizeof(int32_t) * g.total_bins, s);
+    e = cudaMemsetAsync(b.bin_count, 0, sizeof(int32_t) * g.total_bins, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b.bin_fill, 0, sizeof(int32_t) * g.total_bins, s);
+    if (e != cudaSuccess) return cuda_fail(e, "nlb_build_noalloc: clearing the bin tables");
     launch_grid_build(g, d_pos, n, b, s);
     launch_grid_count(g, b, n, cs, counts, s);
   } else {
     launch_brute_count(bp, d_pos, n, cs, counts, s);
   }
   exclusive_scan_u32(counts, n + 1, offs, scan_tmp, s);
-  int64_t total = 0;
-  cudaError_t e = cudaMemcpyAsync(&total, offs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  // Launch-configuration errors are not sticky and a later synchronisation
+  // does not report them: ask for them right after the launches.
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "nlb_build_noalloc count pass launch");
+  // The edge total and the scan's bounded-wait error word, in one sync.
+  int64_t h_tail[2] = {0, 0};
+  e = cudaMemcpyAsync(&h_tail[0], offs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&h_tail[1], scan_tmp + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "nlb_build_noalloc count pass");
+  if (h_tail[1] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+  const int64_t total = h_tail[0];
   *n_edges = total;
   if (total > max_edges)
     return fail(NLB_ERR_VALUE, "nlb_build_noalloc: " + std::to_string(total) +
@@ -232,6 +252,8 @@ Status run_noalloc(const double* d_pos, int64_t n, double cutoff, const double* 
     launch_grid_emit(g, b, n, cs, offs, t, s);
   else
     launch_brute_emit(bp, d_pos, n, cs, offs, t, s);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "nlb_build_noalloc emit pass launch");
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "nlb_build_noalloc emit pass");
   return Status{NLB_OK};

@@ -133,8 +133,10 @@ void plan_grid(const HostCell& c, double rc, GridParams& g) {
     // Bins per axis fit in i32 for any grid whose bin table fits in memory;
     // larger values are clamped and rejected by the caller's size check.
     g.nb[a] = (int32_t)std::min<uint64_t>(nb, (uint64_t)std::numeric_limits<int32_t>::max());
-    total *= (int64_t)g.nb[a];
-    if (total > ((int64_t)1 << 40)) total = ((int64_t)1 << 40);
+    // Saturating product: total stays <= 2^40 (a clamped value only ever
+    // means "too many bins" to the callers' size checks).
+    constexpr int64_t kCap = (int64_t)1 << 40;
+    total = total > kCap / (int64_t)g.nb[a] ? kCap : total * (int64_t)g.nb[a];
   }
   g.total_bins = total;
   for (int a = 0; a < 3; ++a) g.ns[a] = as_i32(std::ceil((rc * (double)g.nb[a]) / w[a]));

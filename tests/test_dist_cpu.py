@@ -62,3 +62,27 @@ def test_reference_arm_prints_once_on_rank0():
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
     assert line["config"]["edges_per_step"] == 490514
     assert line["cpu_baseline"]["cores"] >= 1 and line["cpu_baseline"]["cpu_model"]
+
+
+def test_reference_arm_never_maps_the_product_library():
+    """The CPU reference arm builds its workload without importing the
+    neighborlist_rs package, so the CUDA library is never mapped into it, and
+    it prints the same `config` dict as the GPU arm's bench_config."""
+    code = textwrap.dedent("""
+        import json, sys
+        sys.argv = ["bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0"]
+        import bench
+        bench.main()
+        maps = open("/proc/self/maps").read()
+        print(json.dumps({"mapped": "libnlb200" in maps,
+                          "imported": "neighborlist_rs" in sys.modules}))
+    """)
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(ln) for ln in r.stdout.splitlines() if ln.startswith("{")]
+    line, probe = lines[0], lines[1]
+    assert probe == {"mapped": False, "imported": False}
+    import bench
+
+    assert line["config"] == bench.bench_config(bench.WORKLOAD, 10008, 490514)

@@ -5,6 +5,9 @@ tensors), and each result must equal, edge for edge, what the regular entry
 point nlb_build returns for the same system.  Two different systems are built
 in a row (a periodic cell-list system, then an isolated brute-force one, then
 the first again), so stale contents of the shared scratch array would show.
+The entry point is also checked against the CPU oracle directly, for its
+size checks (refused before any launch), and for the property that defines
+it: a series of calls leaves the device's free memory unchanged.
 This file is collected last on purpose, and it also passes on its own in a
 fresh process.
 """
@@ -91,3 +94,78 @@ def test_noalloc_rejects_oversize(env):
     big = np.random.default_rng(0).random((20000, 3)) * 60.0
     code, m, _, _ = noalloc_build(env, big, None, 5.0, 10)
     assert code == 1 and "fixed capacity" in lib.nlb_last_error().decode()
+
+
+def test_noalloc_matches_oracle(env, oracle):
+    """The entry point against the CPU oracle directly: a periodic cell-list
+    system, an isolated brute-force one and a triclinic cell-list one, each
+    twice in a row."""
+    torch, nl, lib = env
+    from neighborlist_rs import workloads as W
+
+    pos_a, rows_a = W.cluster_liquid(n_clusters=139, box=23.2, seed=41)
+    pos_b = W.isolated_cube(n=900, side=20.0, seed=42)
+    pos_c, rows_c = W.triclinic_uniform(n=4000, seed=43, lengths=(30.0, 36.0))
+    cases = [(pos_a, rows_a, 6.0), (pos_b, None, 5.0), (pos_c, rows_c, 5.0)]
+    for pos, rows, rc in cases + cases:
+        code, m, ei, sh = noalloc_build(env, pos, rows, rc, 300_000)
+        assert code == 0, lib.nlb_last_error().decode()
+        h = None if rows is None else rows.T
+        pbc = None if rows is None else [True] * 3
+        want_ei, want_sh = oracle.search_single(pos, h, pbc, rc, nthreads=4)
+        assert m == want_ei.shape[1] > 0
+        got_ei = torch.stack([ei[0, :m], ei[1, :m]]).cpu().numpy()
+        assert np.array_equal(got_ei, want_ei)
+        assert np.array_equal(sh[:m].cpu().numpy(), want_sh)
+
+
+def test_noalloc_rejects_grids_beyond_capacity_before_launching(env):
+    """A tiny cutoff in a huge cell asks for far more bins than the fixed
+    scratch holds (and more than 2^21 along an axis): the call is refused
+    with NLB_ERR_VALUE before any kernel touches the scratch array."""
+    torch, nl, lib = env
+    pos = np.random.default_rng(5).random((1200, 3)) * 1.0e9
+    rows = np.diag([1.0e9, 1.0e9, 1.0e9])
+    code, m, ei, _ = noalloc_build(env, pos, rows, 1e-3, 10)
+    assert code == 1, lib.nlb_last_error().decode()
+    assert "bins" in lib.nlb_last_error().decode()
+    assert bool((ei == -7).all())
+    # a grid of a few hundred thousand bins: within the per-axis limit, above
+    # the scratch capacity
+    pos = np.random.default_rng(6).random((1200, 3)) * 200.0
+    code, m, _, _ = noalloc_build(env, pos, np.diag([200.0] * 3), 2.5, 10)
+    assert code == 1 and "fixed capacity" in lib.nlb_last_error().decode()
+
+
+def test_noalloc_allocates_no_device_memory(env):
+    """The defining property: once the caller's buffers exist, a series of
+    calls leaves the device's free memory unchanged (no cudaMalloc, no
+    growing workspace)."""
+    torch, nl, lib = env
+    from neighborlist_rs import workloads as W
+
+    pos, rows = W.cluster_liquid(n_clusters=139, box=23.2, seed=44)
+    d_pos = torch.from_numpy(np.ascontiguousarray(pos)).cuda()
+    cap = 200_000
+    ei = torch.empty((2, cap), dtype=torch.int64, device="cuda")
+    sh = torch.empty((cap, 3), dtype=torch.int32, device="cuda")
+    h9 = np.ascontiguousarray(rows.T.reshape(9))
+    h = h9.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    pbc = (ctypes.c_uint8 * 3)(1, 1, 1)
+    m = ctypes.c_int64(-1)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        code = lib.nlb_build_noalloc(d_pos.data_ptr(), pos.shape[0], 6.0, h, pbc,
+                                     ei.data_ptr(), sh.data_ptr(), cap, ctypes.byref(m), stream)
+        assert code == 0, lib.nlb_last_error().decode()
+
+    call()  # the first call on the device looks up the scratch address
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(20):
+        call()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert m.value > 0
