@@ -48,9 +48,6 @@ for _p in (ROOT, PKG_DIR):
 import numpy as np  # noqa: E402
 
 METRIC = "edges/s (exact edges; cluster-liquid N=10008 PBC rc=6)"
-# (cutoff, pass) -> dram__bytes_read.sum + dram__bytes_write.sum per launch.
-NCU_TRAFFIC = {(6.0, "emit"): 4.916e6, (6.0, "count"): 0.454e6,
-               (14.0, "emit"): 129.28e6, (14.0, "count"): 0.446e6}
 UNIT = "edges/s"
 WORKLOAD = "cluster_liquid N=10008 (1112 x 9-atom clusters) cubic L=46.4 A full PBC rc=6.0 A"
 
@@ -187,7 +184,7 @@ def barrier(world):
 # ---------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi samples (200 ms) while the timed region runs."""
+    """nvidia-smi samples (every 100 ms) while the timed region runs."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -202,7 +199,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -270,6 +267,24 @@ def headline_system():
     return pos, rows
 
 
+def ncu_traffic(rc, pass_name):
+    """DRAM bytes (read + write) per launch of the pair-task pass at cutoff rc,
+    and the capture they come from, from the committed ncu traffic table
+    (profiles/ncu_traffic.txt); (None, None) when it has no such row."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                parts = line.split()
+                if not parts or parts[0].startswith("#") or len(parts) < 5:
+                    continue
+                if parts[0] == pass_name and float(parts[1]) == float(rc):
+                    return float(parts[2]) + float(parts[3]), parts[4]
+    except (OSError, ValueError):
+        pass
+    return None, None
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -321,6 +336,19 @@ class DeviceTimer:
         ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
         self.nl.set_stream(self.stream.cuda_stream)
         return ms, edges, launches
+
+    def sustain(self, seconds):
+        """Back-to-back builds for `seconds` of wall time (untimed): keeps the
+        GPU under the same load while the clock sampler records."""
+        t0 = time.perf_counter()
+        k = 0
+        while time.perf_counter() - t0 < seconds:
+            self.step()
+            k += 1
+            if k % 64 == 0:
+                self.torch.cuda.synchronize()
+        self.torch.cuda.synchronize()
+        return k
 
     def phases(self, steps):
         self.nl.profile(True)
@@ -444,8 +472,12 @@ def run_b200(args):
     dt = DeviceTimer(nl, torch, pos, rows, args.rc)
     barrier(world)
     torch.cuda.synchronize()
+    # The timed steps last a few ms, far shorter than the sampler's period: the
+    # sampled window is the timed steps plus 1.5 s of the same builds back to
+    # back right after them.
     with ClockSampler(local) as clk:
         ms, edges, launches = dt.run(args.steps, args.warmup)
+        sustained = dt.sustain(1.5)
     torch.cuda.synchronize()
     barrier(world)
     ms_max = max_over_ranks(ms, world, "cuda")
@@ -461,16 +493,16 @@ def run_b200(args):
     cells = 27  # stencil cells of this grid (n_search = 1 on every axis)
     bytes_emit = 28 * m_step + 48 * n
     bytes_count = 16 * n + 4 * cells * n
-    # The emit pass has the largest share of the ncu launch list
-    # (profiles/k_pair_tasks_cluster_liquid.md); the count pass, within ~2 us
-    # of it in live timing and issue-bound, is reported beside it.
+    # The emit pass has the largest share of the ncu launch list; the count
+    # pass, within a few us of it in live timing and issue-bound, is reported
+    # beside it.
     dominant = "emit"
     alg = bytes_emit
     achieved = alg / (ph[dominant] * 1e-3) / 1e9
     # DRAM bytes (read + write) per launch of the same kernel on the same
-    # workload, from the ncu captures summarised in
-    # profiles/k_pair_tasks_cluster_liquid.md (not measured by this run).
-    traffic = NCU_TRAFFIC.get((float(args.rc), dominant))
+    # workload, from an ncu capture (not measured by this run).
+    traffic, capture = ncu_traffic(args.rc, dominant)
+    count_traffic, _ = ncu_traffic(args.rc, "count")
     kernel_name = {"emit": "k_pair_tasks<1> (emit pass)",
                    "count": "k_pair_tasks<0> (count pass)"}[dominant]
 
@@ -491,18 +523,19 @@ def run_b200(args):
         "config": bench_config(workload, n, m_step),
         "parallelism": f"replicas x{world} (independent systems)",
         "gpu_launches": launches,
-        "clocks": clk.summary(),
+        "clocks": dict(clk.summary(), window=f"timed steps + {sustained} back-to-back builds "
+                                               "(1.5 s) of the same workload"),
         "roofline": {"bound": "hbm", "kernel": kernel_name, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes": alg, "kernel_ms": ph[dominant], "traffic": traffic,
-                     "traffic_source": "ncu capture (profiles/k_pair_tasks_cluster_liquid.md)"
+                     "traffic_source": f"ncu capture {capture} (committed traffic table)"
                      if traffic is not None else None,
                      "phases_ms": ph,
                      "count_pass": {"kernel": "k_pair_tasks<0> (count pass)",
                                     "bound": "instruction issue (61-78 % issue-active in ncu)",
                                     "algorithmic_bytes": bytes_count, "kernel_ms": ph["count"],
                                     "achieved_gbs": bytes_count / (ph["count"] * 1e-3) / 1e9,
-                                    "traffic": NCU_TRAFFIC.get((float(args.rc), "count"))}},
+                                    "traffic": count_traffic}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n + 72,
                 "d2h_bytes_per_step": 28 * m_e2e},
     }

@@ -144,6 +144,18 @@ void nlb_set_stream(void* stream);
 /* Kernel launches issued by this library since load (all threads). */
 int64_t nlb_kernel_launches(void);
 
+/* Failure-detection hook (no counterpart in the reference, which has no
+ * device waits).  The device prefix scans wait on their predecessor tiles
+ * with bounded polls; when a wait runs out, the scan records an error word,
+ * finishes without waiting further, the emit pass writes nothing, and the
+ * build returns NLB_ERR_CUDA ("prefix scan gave up waiting for a tile") with
+ * the device and the library still usable.  This call makes the calling
+ * thread's next scan launch exercise that path: its tile `tile` withholds
+ * its publication, and its successors poll at most spin_limit times.  One
+ * shot; builds whose scan has fewer tiles are unaffected.  Returns NLB_OK,
+ * or NLB_ERR_VALUE for tile < 0 or spin_limit < 1. */
+int nlb_debug_scan_stall(int32_t tile, int32_t spin_limit);
+
 /* Per-thread phase timing with CUDA events on the launching stream.
  * enable != 0 starts (and resets) it.  nlb_profile_read fills ms[0..3] with
  * the accumulated device time of: grid build, count pass, offset scan, emit
@@ -282,11 +294,20 @@ int nlb_build_noalloc(const double* d_positions, int64_t n_atoms, double cutoff,
  *   the ticket is retired; device results stay owned by the server until
  *   nlb_server_release, which the caller issues once its own work reading
  *   them has completed.
- * nlb_server_stats: fills 13 counters: submitted, completed, failed, batches,
+ * nlb_server_stats: fills 14 counters: submitted, completed, failed, batches,
  *   HBM bytes reserved, queued requests, largest batch, budget, then worker
  *   wall time in microseconds (all workers) spent in: batch staging and
  *   launches, waiting for the count pass, issuing result copies, waiting
- *   for the emit pass and copies, large requests.
+ *   for the emit pass and copies, large requests; then cancelled requests.
+ * nlb_server_pause: paused != 0 stops the workers from taking new work
+ *   (requests queue up, running work finishes); 0 resumes.
+ * nlb_server_cancel: withdraws a queued request (it never runs) or frees a
+ *   finished request's result; the ticket is retired either way.  A running
+ *   request cannot be cancelled (NLB_ERR_VALUE, "request still running").
+ * nlb_server_debug_fail: failure-detection hook for tests: the staging of
+ *   any batch holding this queued request fails as if a CUDA call had
+ *   returned an error; the worker reruns that batch one request at a time,
+ *   so only this request fails (NLB_ERR_CUDA) and the others complete.
  * nlb_server_destroy: cancels queued requests, lets running ones finish,
  *   joins the workers (freeing their workspaces) and frees every result that
  *   was not handed over.  No thread may be inside nlb_server_wait then. */
@@ -298,6 +319,9 @@ int64_t nlb_server_submit(nlb_server* server, const double* positions, int64_t n
 int nlb_server_wait(nlb_server* server, int64_t ticket, double timeout_s, nlb_result* out,
                     double* latency_ms);
 int nlb_server_release(nlb_server* server, int64_t ticket);
+int nlb_server_pause(nlb_server* server, int paused);
+int nlb_server_cancel(nlb_server* server, int64_t ticket);
+int nlb_server_debug_fail(nlb_server* server, int64_t ticket);
 void nlb_server_stats(nlb_server* server, int64_t* stats);
 void nlb_server_destroy(nlb_server* server);
 

@@ -51,10 +51,12 @@ constexpr int kMaxDevices = 64;
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Scan state for the largest scans here (n + 1 counts, a bin histogram).
+// Scan states for the largest scans here: the n + 1 counts in the first
+// half, the bin histogram in the second (each keeps its own error word).
 constexpr int64_t kNoAllocScanWords = 64;
-static_assert((kNoAllocMaxAtoms + 1 + kScanTile - 1) / kScanTile + 2 <= kNoAllocScanWords &&
-                  (kNoAllocMaxBins + kScanTile - 1) / kScanTile + 2 <= kNoAllocScanWords,
+constexpr int64_t kNoAllocBinScan = kNoAllocScanWords / 2;
+static_assert((kNoAllocMaxAtoms + 1 + kScanTile - 1) / kScanTile + 2 <= kNoAllocBinScan &&
+                  (kNoAllocMaxBins + kScanTile - 1) / kScanTile + 2 <= kNoAllocBinScan,
               "scan state of the scratch array too small for the scan tile");
 
 // Byte layout of the scratch array (each piece 256-byte aligned).
@@ -191,7 +193,7 @@ Status run_noalloc(const double* d_pos, int64_t n, double cutoff, const double* 
     b.py = at<double>(base, kLayout.py);
     b.pz = at<double>(base, kLayout.pz);
     b.meta = at<SlotMeta>(base, kLayout.meta);
-    b.scan_tmp = at<int64_t>(base, kLayout.scan_tmp);
+    b.scan_tmp = at<int64_t>(base, kLayout.scan_tmp) + kNoAllocBinScan;
   } else {
     std::memcpy(bp.h, cell.h, sizeof(bp.h));
     std::memcpy(bp.hinv, cell.hinv, sizeof(bp.hinv));
@@ -224,14 +226,17 @@ Status run_noalloc(const double* d_pos, int64_t n, double cutoff, const double* 
   // does not report them: ask for them right after the launches.
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "nlb_build_noalloc count pass launch");
-  // The edge total and the scan's bounded-wait error word, in one sync.
-  int64_t h_tail[2] = {0, 0};
+  // The edge total and the scans' bounded-wait error words, in one sync.
+  int64_t h_tail[3] = {0, 0, 0};
   e = cudaMemcpyAsync(&h_tail[0], offs + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&h_tail[1], scan_tmp + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && method == Method::kCellList)
+    e = cudaMemcpyAsync(&h_tail[2], b.scan_tmp + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "nlb_build_noalloc count pass");
-  if (h_tail[1] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+  if (h_tail[1] != 0 || h_tail[2] != 0)
+    return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
   const int64_t total = h_tail[0];
   *n_edges = total;
   if (total > max_edges)

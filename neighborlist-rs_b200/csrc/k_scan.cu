@@ -7,7 +7,11 @@
 // warp walks back over the predecessors' published aggregates / inclusive
 // prefixes 32 at a time until it meets an inclusive prefix.  Every wait is
 // bounded: after kSpinLimit polls the CTA records an error in the state
-// buffer (word 1, read back by the host) and stops waiting.  HBM-bound:
+// buffer (word 1, read back by the host) and stops waiting.  A failure-
+// detection hook (nlb_debug_scan_stall) makes one tile of the calling
+// thread's next scan withhold its publication, with a short poll limit, so
+// that the bounded wait and its error report can be exercised without any
+// fault: the successors give up, record the error and finish.  HBM-bound:
 // 4 B read + 8 B written per element.  The state buffer (tiles + 2 words) is
 // zeroed by a memset node right before the kernel.
 #include "nlb_kernels.h"
@@ -22,6 +26,11 @@ constexpr int kItems = kTile / kThreads;
 static_assert(kItems * kThreads == kTile, "tile = threads x items");
 constexpr int kPadShift = 5;              // one padding word per 32 elements
 constexpr int kSpinLimit = 1 << 22;
+
+// One-shot failure-detection hook of the calling host thread (see
+// nlb_debug_scan_stall): tile to withhold in the next scan and its poll limit.
+thread_local int32_t tl_withhold_tile = -1;
+thread_local int32_t tl_withhold_spins = 0;
 
 constexpr uint64_t kStatusShift = 62;
 constexpr uint64_t kAggregate = 1ull << kStatusShift;
@@ -42,7 +51,7 @@ __device__ __forceinline__ void store_state(uint64_t* p, uint64_t v) {
 template <class TIn>
 __global__ void __launch_bounds__(kThreads)
     k_scan(const TIn* __restrict__ in, int64_t n, int64_t* __restrict__ out,
-           uint64_t* __restrict__ state) {
+           uint64_t* __restrict__ state, int32_t withhold, int32_t spin_limit) {
   // state[0]: tile ticket counter; state[1]: error flag; state[2 + t]: tile t.
   __shared__ uint32_t stage_in[kTile + kTile / 32];
   __shared__ int64_t warp_sums[kThreads / 32];
@@ -97,10 +106,13 @@ __global__ void __launch_bounds__(kThreads)
   if (warp == 0) {
     uint64_t* tiles = state + 2;
     int64_t prefix = 0;
+    const bool publish = tile != withhold;  // false only under the test hook
     if (tile == 0) {
-      if (lane == 0) store_state(&tiles[0], kInclusive | ((uint64_t)aggregate & kValueMask));
+      if (lane == 0 && publish)
+        store_state(&tiles[0], kInclusive | ((uint64_t)aggregate & kValueMask));
     } else {
-      if (lane == 0) store_state(&tiles[tile], kAggregate | ((uint64_t)aggregate & kValueMask));
+      if (lane == 0 && publish)
+        store_state(&tiles[tile], kAggregate | ((uint64_t)aggregate & kValueMask));
       int t = tile - 1;
       for (;;) {
         const int pred = t - lane;  // lane 0 = nearest predecessor
@@ -109,7 +121,7 @@ __global__ void __launch_bounds__(kThreads)
         if (pred >= 0) {
           int spins = 0;
           v = load_state(&tiles[pred]);
-          while ((v >> kStatusShift) == 0 && spins < kSpinLimit) {
+          while ((v >> kStatusShift) == 0 && spins < spin_limit) {
             __nanosleep(32);
             v = load_state(&tiles[pred]);
             ++spins;
@@ -130,7 +142,7 @@ __global__ void __launch_bounds__(kThreads)
         if (stop >= 0) break;
         t -= 32;
       }
-      if (lane == 0)
+      if (lane == 0 && publish)
         store_state(&tiles[tile], kInclusive | ((uint64_t)(prefix + aggregate) & kValueMask));
     }
     if (lane == 0) s_prefix = prefix;
@@ -171,12 +183,22 @@ void scan_impl(const TIn* in, int64_t n, int64_t* out, int64_t* tmp, cudaStream_
                bool zero_state = true) {
   const int64_t tiles = n > 0 ? (n + kTile - 1) / kTile : 1;
   if (zero_state) cudaMemsetAsync(tmp, 0, sizeof(int64_t) * (size_t)(tiles + 2), s);
+  const int32_t withhold = tl_withhold_tile;
+  const int32_t spins = withhold >= 0 ? tl_withhold_spins : kSpinLimit;
+  tl_withhold_tile = -1;
   launch_pdl(k_scan<TIn>, dim3((unsigned)tiles), dim3(kThreads), 0, s, in, n, out,
-             reinterpret_cast<uint64_t*>(tmp));
+             reinterpret_cast<uint64_t*>(tmp), withhold, spins);
   note_launches(1);
 }
 
 }  // namespace
+
+bool scan_stall_armed() { return tl_withhold_tile >= 0; }
+
+void arm_scan_stall(int32_t tile, int32_t spin_limit) {
+  tl_withhold_tile = tile;
+  tl_withhold_spins = spin_limit;
+}
 
 int64_t scan_tmp_elems(int64_t n) { return (n > 0 ? (n + kTile - 1) / kTile : 1) + 2; }
 

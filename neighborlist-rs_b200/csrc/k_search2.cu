@@ -222,6 +222,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? (K == 1 ? 3 : 1) : (K 
   SlotMeta* smt = stage_m[warp];
   pdl_wait();
   int64_t* dst0 = EMIT ? t.dst[0] : nullptr;
+  if (EMIT && t.scan_error && *t.scan_error != 0) return;  // offsets not valid
   if (EMIT && t.total_dev) {
     const int64_t m_total = *t.total_dev;
     if (m_total > t.capacity) return;  // the caller grows the arena and emits again

@@ -409,8 +409,11 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
   sp.row = row;
   sp.counts = slot<uint32_t>(c, kSlotCounts, (size_t)k * row);
   sp.offs = slot<int64_t>(c, kSlotOffs, (size_t)k * row + 1);
+  // Offsets-scan state, then a separate state for the bin scan of grids too
+  // large for k_prep's own (so that each keeps its own error word).
+  const int64_t offs_state = scan_tmp_elems((int64_t)k * row);
   int64_t* scan_tmp = slot<int64_t>(
-      c, kSlotScanTmp, (size_t)scan_tmp_elems(std::max<int64_t>((int64_t)k * row, sp.grid.total_bins)));
+      c, kSlotScanTmp, (size_t)(offs_state + scan_tmp_elems(sp.grid.total_bins)));
   if (!sp.counts || !sp.offs || !scan_tmp) return fail(NLB_ERR_NOMEM, "device allocation failed");
 
   c.mark(0);
@@ -442,7 +445,7 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
     b.py = slot<double>(c, kSlotPy, n);
     b.pz = slot<double>(c, kSlotPz, n);
     b.meta = slot<SlotMeta>(c, kSlotMeta, n);
-    b.scan_tmp = scan_tmp;
+    b.scan_tmp = scan_tmp + offs_state;
     b.p32 = nullptr;
     b.sbin = nullptr;
     b.groups = nullptr;
@@ -497,7 +500,7 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
   exclusive_scan_u32(sp.counts, (int64_t)k * row, sp.offs, scan_tmp, s);
   c.mark(3);
   // Row starts offs[q * row], q = 0..k, in one strided copy.
-  if (k + 3 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
+  if (k + 4 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
   cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), sp.offs, sizeof(int64_t) * row,
                                     sizeof(int64_t), (size_t)k + 1, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)  // the scan's bounded-wait error word
@@ -506,10 +509,17 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
   if (e == cudaSuccess && pair_tasks)  // hit-mask words the count pass asked for
     e = cudaMemcpyAsync(c.h_small + k + 2, sp.gb.mask_top, sizeof(int64_t),
                         cudaMemcpyDeviceToHost, s);
+  const bool bin_scan = sp.method == Method::kCellList &&
+                        !(sp.gb.build_done && sp.grid.total_bins <= kFusedBinScanMax);
+  c.h_small[k + 3] = 0;
+  if (e == cudaSuccess && bin_scan)  // the separate bin scan's error word
+    e = cudaMemcpyAsync(c.h_small + k + 3, sp.gb.scan_tmp + 1, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy2DAsync");
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "count pass");
-  if (c.h_small[k + 1] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+  if (c.h_small[k + 1] != 0 || c.h_small[k + 3] != 0)
+    return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
   if (c.prof) {
     c.harvest();  // a previous emit on this stream is complete too
     c.prof_pending_count = true;
@@ -1106,6 +1116,14 @@ int nlb_copy_device(void* dst, const void* src, size_t bytes, void* stream) {
 void nlb_set_stream(void* stream) { tl_user_stream = static_cast<cudaStream_t>(stream); }
 
 int64_t nlb_kernel_launches(void) { return g_launches.load(); }
+
+int nlb_debug_scan_stall(int32_t tile, int32_t spin_limit) {
+  if (tile < 0 || spin_limit < 1)
+    return fail(NLB_ERR_VALUE, "nlb_debug_scan_stall: tile must be >= 0 and spin_limit >= 1")
+        .code;
+  arm_scan_stall(tile, spin_limit);
+  return NLB_OK;
+}
 
 void nlb_profile(int enable) {
   tl_profile = enable != 0;

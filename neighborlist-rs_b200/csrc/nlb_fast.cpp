@@ -147,6 +147,7 @@ EmitTargets fast_targets(const SystemPlan& sp, int64_t capacity) {
   t.sh[0] = sp.out_sh;
   t.total_dev = sp.offs + sp.row;
   t.capacity = capacity;
+  t.scan_error = sp.scan_state + 1;
   return t;
 }
 
@@ -199,7 +200,10 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
   key.need_rank = sp.rank_cached ? 0 : 1;
   key.prof = c.prof ? 1 : 0;
 
-  const bool same = fs.have_key && std::memcmp(&key, &fs.key, sizeof(key)) == 0;
+  // (An armed failure-detection hook must reach a directly launched scan,
+  // never a captured or replayed one.)
+  const bool same = !scan_stall_armed() && fs.have_key &&
+                    std::memcmp(&key, &fs.key, sizeof(key)) == 0;
   bool launched = false;
   if (same && fs.exec) {
     if (cudaGraphLaunch(fs.exec, c.stream) == cudaSuccess) {
@@ -250,9 +254,16 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(c.h_small + 2, sp.gb.mask_top, sizeof(int64_t), cudaMemcpyDeviceToHost,
                         c.stream);
+  // Grids too large for k_prep's own bin scan use a separate scan (state in
+  // gb.scan_tmp): its error word too.
+  c.h_small[3] = 0;
+  if (e == cudaSuccess && sp.grid.total_bins > kFusedBinScanMax)
+    e = cudaMemcpyAsync(c.h_small + 3, sp.gb.scan_tmp + 1, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, c.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
   if (e != cudaSuccess) return cuda_fail(e, "neighbour-list pipeline");
-  if (c.h_small[1] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+  if (c.h_small[1] != 0 || c.h_small[3] != 0)
+    return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
   const int64_t m = c.h_small[0];
   if (c.prof) {
     c.prof_pending_count = true;

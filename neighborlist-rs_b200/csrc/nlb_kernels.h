@@ -14,6 +14,11 @@ namespace nlb {
 // scan_tmp_elems(n) = ceil(n / kScanTile) + 2 int64 elements.
 constexpr int64_t kScanTile = 2048;  // elements per CTA (measured best of 1024-4096)
 int64_t scan_tmp_elems(int64_t n);
+// Failure-detection hook: the calling thread's next scan launch has `tile`
+// withhold its publication and its successors poll at most spin_limit times
+// (then record the error word and finish).  One-shot.
+void arm_scan_stall(int32_t tile, int32_t spin_limit);
+bool scan_stall_armed();
 void exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, int64_t* tmp,
                         cudaStream_t s);
 void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* tmp,
@@ -104,6 +109,9 @@ struct EmitTargets {
   // nothing is written if M > capacity (the caller grows and re-emits).
   const int64_t* total_dev;
   int64_t capacity;
+  // Pair-task emit only: when set and non-zero (the offsets scan gave up
+  // waiting for a tile), nothing is written: the offsets are not valid.
+  const int64_t* scan_error;
   // Batched kernels: 1 = atom indices local to each system (served requests),
   // 0 = global indices (system start added).
   int32_t local_indices;

@@ -61,6 +61,7 @@ struct Req {
   int64_t* ei = nullptr;  // [src | dst]
   int32_t* sh = nullptr;
   void* dev_block = nullptr;  // device result: the batch block ei/sh point into
+  bool fail_staging = false;  // failure-detection hook: the staging of any batch holding it fails
 };
 
 // Result bytes one batch of small requests may produce (estimated): bounds
@@ -277,6 +278,50 @@ class Server {
     return NLB_OK;
   }
 
+  // Workers take no new work while paused (requests queue up; running work
+  // finishes).
+  void pause(bool paused) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      paused_ = paused;
+    }
+    cv_work_.notify_all();
+  }
+
+  // Withdraws a request: a queued one leaves the queue, a finished one has
+  // its result freed; either way the ticket is retired.  A running request
+  // cannot be withdrawn (NLB_ERR_VALUE, "request still running").
+  int cancel(int64_t id) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) return fail(NLB_ERR_VALUE, "unknown ticket").code;
+    Req* r = it->second;
+    if (r->status == 1) return fail(NLB_ERR_VALUE, "request still running").code;
+    if (r->status == 0) {
+      queue_.erase(std::find(queue_.begin(), queue_.end(), r));
+      ++cancelled_;
+    }
+    in_use_ -= r->result_bytes;
+    r->result_bytes = 0;
+    reqs_.erase(it);
+    free_req(r);
+    cv_work_.notify_all();
+    return NLB_OK;
+  }
+
+  // Failure-detection hook: the staging of any batch that holds this queued
+  // request fails (as if a CUDA call of the staging had returned an error),
+  // so the worker reruns the batch one request at a time and only this
+  // request fails.
+  int debug_fail(int64_t id) {
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) return fail(NLB_ERR_VALUE, "unknown ticket").code;
+    if (it->second->status != 0) return fail(NLB_ERR_VALUE, "request not queued").code;
+    it->second->fail_staging = true;
+    return NLB_OK;
+  }
+
   int release(int64_t id) {
     std::lock_guard<std::mutex> lk(mu_);
     auto it = reqs_.find(id);
@@ -313,6 +358,7 @@ class Server {
     s[10] = us_deliver.load();
     s[11] = us_emit_wait.load();
     s[12] = us_large.load();
+    s[13] = cancelled_;
   }
 
  private:
@@ -383,7 +429,7 @@ class Server {
         std::unique_lock<std::mutex> lk(mu_);
         cv_work_.wait(lk, [&] {
           if (stop_) return true;
-          if (queue_.empty()) return false;
+          if (paused_ || queue_.empty()) return false;
           return in_use_ + queue_.front()->est_bytes <= budget_;
         });
         if (stop_) break;
@@ -472,6 +518,7 @@ class Server {
   }
 
   Status run_large(Req* r) {
+    if (r->fail_staging) return fail(NLB_ERR_CUDA, "request staging failed (injected)");
     Ctx* c = nullptr;
     Status st = get_ctx(&c);
     if (!st.ok()) return st;
@@ -514,6 +561,8 @@ class Server {
   }
 
   Status run_batch_items(std::vector<Req*>& items) {
+    for (Req* r : items)
+      if (r->fail_staging) return fail(NLB_ERR_CUDA, "batch staging failed (injected)");
     Ctx* c = nullptr;
     Status st = get_ctx(&c);
     if (!st.ok()) return st;
@@ -747,6 +796,8 @@ class Server {
   std::unordered_map<int64_t, Req*> reqs_;
   size_t in_use_ = 0;
   bool stop_ = false;
+  bool paused_ = false;
+  int64_t cancelled_ = 0;
   int64_t next_id_ = 1;
   int64_t submitted_ = 0, completed_ = 0, failed_ = 0, batches_ = 0, max_batch_seen_ = 0;
   std::vector<std::thread> threads_;
@@ -806,6 +857,22 @@ int nlb_server_wait(nlb_server* s, int64_t ticket, double timeout_s, nlb_result*
 int nlb_server_release(nlb_server* s, int64_t ticket) {
   if (!s) return nlb::fail(NLB_ERR_VALUE, "server is NULL").code;
   return s->impl->release(ticket);
+}
+
+int nlb_server_pause(nlb_server* s, int paused) {
+  if (!s) return nlb::fail(NLB_ERR_VALUE, "server is NULL").code;
+  s->impl->pause(paused != 0);
+  return NLB_OK;
+}
+
+int nlb_server_cancel(nlb_server* s, int64_t ticket) {
+  if (!s) return nlb::fail(NLB_ERR_VALUE, "server is NULL").code;
+  return s->impl->cancel(ticket);
+}
+
+int nlb_server_debug_fail(nlb_server* s, int64_t ticket) {
+  if (!s) return nlb::fail(NLB_ERR_VALUE, "server is NULL").code;
+  return s->impl->debug_fail(ticket);
 }
 
 void nlb_server_stats(nlb_server* s, int64_t* stats) {

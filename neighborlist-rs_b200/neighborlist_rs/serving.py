@@ -30,12 +30,15 @@ _lib.nlb_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_doubl
                                  ctypes.POINTER(_Result), ctypes.POINTER(ctypes.c_double)]
 _lib.nlb_server_release.argtypes = [ctypes.c_void_p, ctypes.c_int64]
 _lib.nlb_server_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
+_lib.nlb_server_pause.argtypes = [ctypes.c_void_p, ctypes.c_int]
+_lib.nlb_server_cancel.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+_lib.nlb_server_debug_fail.argtypes = [ctypes.c_void_p, ctypes.c_int64]
 _lib.nlb_server_destroy.argtypes = [ctypes.c_void_p]
 
 _NLB_NOT_READY = 4
 _STATS = ("submitted", "completed", "failed", "batches", "reserved_bytes", "queued",
           "largest_batch", "budget_bytes", "us_stage", "us_count_wait", "us_deliver",
-          "us_emit_wait", "us_large")
+          "us_emit_wait", "us_large", "cancelled")
 
 
 class DeviceResult:
@@ -137,6 +140,24 @@ class Server:
 
     def wait(self, ticket: int, timeout: float | None = None):
         return self.wait_timed(ticket, timeout)[0]
+
+    def pause(self, paused: bool = True) -> None:
+        """Stops (or resumes) the workers taking new work; queued requests
+        wait, running work finishes."""
+        _check(_lib.nlb_server_pause(self._handle(), int(bool(paused))))
+
+    def cancel(self, ticket: int) -> None:
+        """Withdraws a queued request (it never runs) or frees a finished
+        one's result; the ticket is retired.  Raises ValueError for a running
+        request or an unknown ticket."""
+        _check(_lib.nlb_server_cancel(self._handle(), int(ticket)))
+        with self._lock:
+            self._device_tickets.discard(int(ticket))
+
+    def _debug_fail(self, ticket: int) -> None:
+        """Failure-detection hook for tests: the staging of any batch holding
+        this queued request fails; only this request reports the error."""
+        _check(_lib.nlb_server_debug_fail(self._handle(), int(ticket)))
 
     def stats(self) -> dict:
         buf = (ctypes.c_int64 * len(_STATS))()

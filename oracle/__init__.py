@@ -277,3 +277,21 @@ def edge_extras(positions, h, edges, directed=False):
                           _dp(dist))
     return (ei_out[: 2 * mo].reshape(2, mo), sh_out[: 3 * mo].reshape(mo, 3),
             vec[: 3 * mo].reshape(mo, 3), dist[:mo])
+
+
+def verlet_filter(positions, h, edges, cutoff):
+    """The filter step of the skin-list manager (no counterpart in the
+    reference, whose spec.md:41-48 and 209-222 only describe it): the stored
+    half list (i, j, S), built at cutoff + skin from the positions of the last
+    rebuild, is kept in stored order where |(r_j - r_i) + H.S|^2 < cutoff^2
+    with the current positions.  The displacement is edge_extras'
+    expression; the squared norm is (d0^2 + d1^2) + d2^2, each operation a
+    separately rounded FP64 multiply or add (numpy never fuses them).
+    h=None: a system without a cell (d = r_j - r_i)."""
+    ei, sh = edges
+    if ei.shape[1] == 0:
+        return ei.copy(), sh.copy()
+    _, _, vec, _ = edge_extras(positions, h, edges)
+    n2 = (vec[:, 0] * vec[:, 0] + vec[:, 1] * vec[:, 1]) + vec[:, 2] * vec[:, 2]
+    keep = n2 < float(cutoff) * float(cutoff)
+    return np.ascontiguousarray(ei[:, keep]), np.ascontiguousarray(sh[keep])

@@ -32,3 +32,29 @@ def test_vectors_follow_shift_convention(oracle):
     m = ei.shape[1]
     assert np.array_equal(full[0][:, m:], ei[::-1]) and np.array_equal(full[1][m:], -sh)
     assert np.array_equal(full[2][m:], -vec) and np.array_equal(full[3][m:], dist)
+
+
+def test_verlet_filter_restatement(oracle):
+    """oracle.verlet_filter on known answers: for an isolated brute-force
+    system (raw positions, d = r_j - r_i in both computations) filtering the
+    list at rc + skin down to rc gives exactly the oracle's list at rc, in
+    order; for a periodic system it gives the same pair set away from rc."""
+    rng = np.random.default_rng(8)
+    pos = rng.random((400, 3)) * 16.0
+    wide = oracle.search_single(pos, None, None, 5.0)
+    got = oracle.verlet_filter(pos, None, wide, 4.0)
+    want = oracle.search_single(pos, None, None, 4.0)
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+    h = np.eye(3) * 14.0
+    pos = rng.random((1200, 3)) * 14.0
+    wide = oracle.search_single(pos, h, [True] * 3, 5.0)
+    got = oracle.verlet_filter(pos, h, wide, 4.0)
+    want = oracle.search_single(pos, h, [True] * 3, 4.0)
+    as_set = lambda e: set(zip(e[0][0].tolist(), e[0][1].tolist(), map(tuple, e[1].tolist())))
+    assert as_set(got) == as_set(want)
+    # moved positions: exactly the stored pairs now inside rc, stored order kept
+    moved = pos + rng.normal(0.0, 0.05, pos.shape)
+    got = oracle.verlet_filter(moved, h, wide, 4.0)
+    d = moved[wide[0][1]] - moved[wide[0][0]] + wide[1] @ h.T
+    keep = (d * d).sum(axis=1) < 16.0
+    assert np.array_equal(got[0], wide[0][:, keep]) and np.array_equal(got[1], wide[1][keep])

@@ -404,9 +404,10 @@ def test_torch_device_api(nl, oracle):
 
 
 def test_far_images_take_full_transfer(nl, oracle):
-    """Host-bound lists travel in a compact form whose shifts hold
-    [-511, 511]; atoms hundreds of cells away from the box give larger
-    shifts, so that call falls back to the full form -- same result."""
+    """The count pass stores a task's image shift in three 10-bit fields
+    ([-511, 511]) beside its hit masks; atoms hundreds of cells away from the
+    box give larger shifts, so those tasks skip the masks and the emit pass
+    recomputes their tests -- same result."""
     from neighborlist_rs import workloads as W
 
     pos, rows = W.cluster_liquid(n_clusters=200, box=26.0, seed=5)
