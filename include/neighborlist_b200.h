@@ -133,6 +133,25 @@ typedef struct nlb_device_result {
 int nlb_build_device(const double* d_positions, int64_t n_atoms, double cutoff,
                      const double* cell, const uint8_t* pbc, nlb_device_result* out);
 
+/* Zero-copy device results (no counterpart in the reference, whose results
+ * are host Vecs; its consumer is a GNN that takes edge_index on the GPU,
+ * spec.md:13).  As nlb_build_device, but the two result arrays are handed
+ * over to the caller: they are device blocks of the library's stream-ordered
+ * result pool, written in place by the build (no copy), and stay valid until
+ * the caller returns each one with nlb_device_free.  Both are NULL when
+ * M = 0.  The blocks may be larger than 16 M and 12 M bytes; edge_index is
+ * [src | dst] in its first 2 M entries.
+ * nlb_device_free: returns such a block to the pool after the work queued so
+ * far on `stream` (a cudaStream_t; NULL = legacy default stream): pass the
+ * stream whose work last used the block.  NLB_ERR_VALUE for a pointer that is
+ * not an outstanding block.
+ * nlb_device_blocks: out3 = {blocks handed out, blocks returned, bytes of the
+ * blocks still outstanding}. */
+int nlb_build_device_owned(const double* d_positions, int64_t n_atoms, double cutoff,
+                           const double* cell, const uint8_t* pbc, nlb_device_result* out);
+int nlb_device_free(void* p, void* stream);
+void nlb_device_blocks(int64_t* out3);
+
 /* Device-to-device copy on `stream` (a cudaStream_t): lets callers move a
  * device result into memory they own before the next build. */
 int nlb_copy_device(void* dst, const void* src, size_t bytes, void* stream);
@@ -143,6 +162,11 @@ void nlb_set_stream(void* stream);
 
 /* Kernel launches issued by this library since load (all threads). */
 int64_t nlb_kernel_launches(void);
+/* CUDA-graph replays since load (all threads): a repeated identical
+ * single-system build (same sizes, cell, cutoff, buffers, stream) and a
+ * repeated batched build of the same shape (same system sizes, cutoffs,
+ * decided launch shape, buffers, stream) replay their captured graphs. */
+int64_t nlb_graph_replays(void);
 
 /* Failure-detection hook (no counterpart in the reference, which has no
  * device waits).  The device prefix scans wait on their predecessor tiles

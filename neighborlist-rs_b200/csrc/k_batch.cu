@@ -170,7 +170,10 @@ __global__ void k_plan(const double* __restrict__ pos, const int64_t* __restrict
     P.method = 2;
     dev_plan_grid(w, rc_max, g);
     for (int a = 0; a < 3; ++a)
-      if (g.ns[a] < 0 || g.ns[a] > (1 << 20)) atomicExch(error_flag, 2);
+      if (g.ns[a] < 0 || g.ns[a] > (1 << 20)) {
+        atomicExch(error_flag, 2);
+        P.method = -1;  // (the host reports it; the passes skip the system)
+      }
   }
   plans[s - s0] = P;
 }
@@ -500,6 +503,14 @@ __global__ void __launch_bounds__(THREADS)
   const SmemView v = smem_view(smem, cap);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool blocks = t.system_blocks && cs.k == 0;
+  // Device-sized outputs: nothing is written when the offsets scan gave up,
+  // or when any list of this pass holds more edges than the arena (the host
+  // grows the arena and emits again).
+  if (t.scan_error && *t.scan_error != 0) return;
+  if (t.capacity > 0) {
+    for (int q = 0; q < cs.k; ++q)
+      if (offs[(int64_t)(q + 1) * row] - offs[(int64_t)q * row] > t.capacity) return;
+  }
   for (;;) {
     const int2 item = next_item(work, items, n_items);
     if (item.x < 0) break;

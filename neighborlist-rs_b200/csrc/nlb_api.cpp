@@ -48,6 +48,8 @@ std::atomic<uint64_t> g_stack_threshold{1000};  // DEFAULT_STACK_THRESHOLD
 
 std::atomic<int64_t> g_launches{0};
 void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+std::atomic<int64_t> g_graph_replays{0};
+void note_graph_replay() { g_graph_replays.fetch_add(1, std::memory_order_relaxed); }
 
 thread_local cudaStream_t tl_user_stream = nullptr;
 
@@ -290,8 +292,92 @@ void pinned_stats(int64_t* out) {
 
 // ------------------------------------------------------------------ context
 
+namespace {
+
+// Per-device stream-ordered pool of the single-system result arrays, so that
+// a build can hand its arrays to the caller (nlb_build_device_owned) and the
+// next build gets fresh ones without cudaMalloc's device-wide cost.  Memory
+// stays mapped in the pool (release threshold: unlimited).
+struct ResultPool {
+  std::mutex mu;
+  cudaMemPool_t pool[64] = {};
+  // Blocks handed to callers: pointer -> (device, bytes).
+  std::unordered_map<void*, std::pair<int, size_t>> owned;
+  int64_t handed = 0, returned = 0;
+};
+
+ResultPool& result_pool() {
+  static ResultPool* p = new ResultPool();  // process lifetime
+  return *p;
+}
+
+cudaMemPool_t result_pool_for(int dev) {
+  ResultPool& rp = result_pool();
+  if (dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(rp.mu);
+  if (!rp.pool[dev]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    rp.pool[dev] = pool;
+  }
+  return rp.pool[dev];
+}
+
+bool is_result_slot(int slot) { return slot == kSlotOutEi || slot == kSlotOutSh; }
+
+}  // namespace
+
+void take_result_arrays(Ctx& c, int64_t** ei, int32_t** sh) {
+  ResultPool& rp = result_pool();
+  std::lock_guard<std::mutex> lk(rp.mu);
+  Ctx::Buf* bs[2] = {&c.bufs[kSlotOutEi], &c.bufs[kSlotOutSh]};
+  for (Ctx::Buf* b : bs) {
+    if (b->p) {
+      rp.owned[b->p] = {c.device, b->cap};
+      ++rp.handed;
+    }
+  }
+  *ei = static_cast<int64_t*>(bs[0]->p);
+  *sh = static_cast<int32_t*>(bs[1]->p);
+  *bs[0] = Ctx::Buf{};
+  *bs[1] = Ctx::Buf{};
+}
+
 void* Ctx::raw(int slot, size_t bytes) {
   Buf& b = bufs[slot];
+  if (bytes > b.cap && is_result_slot(slot)) {
+    // Result arrays come from the stream-ordered pool.  Growth waits for the
+    // device first (the old array may still be in use on another stream, as
+    // a cudaFree would).
+    if (b.p) {
+      cudaDeviceSynchronize();
+      if (b.pooled)
+        cudaFreeAsync(b.p, stream);
+      else
+        cudaFree(b.p);
+    }
+    b = Buf{};
+    const size_t cap = std::max<size_t>(bytes + bytes / 4, 4096);
+    cudaMemPool_t pool = result_pool_for(device);
+    if (!pool || cudaMallocFromPoolAsync(&b.p, cap, pool, stream) != cudaSuccess) {
+      cudaGetLastError();
+      b = Buf{};
+      return nullptr;
+    }
+    b.cap = cap;
+    b.pooled = true;
+    return b.p;
+  }
   if (bytes > b.cap) {
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
@@ -313,14 +399,20 @@ thread_local std::unordered_map<int, Ctx*> tl_ctxs;
 
 void release_thread_ctx() {
   release_fast_states();
+  release_batch_graphs();
   for (auto& kv : tl_ctxs) {
     Ctx* c = kv.second;
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    for (Ctx::Buf& b : c->bufs) {
+      if (b.p && b.pooled)
+        cudaFreeAsync(b.p, c->own_stream);
+      else if (b.p)
+        cudaFree(b.p);
+    }
     cudaStreamSynchronize(c->own_stream);
-    for (Ctx::Buf& b : c->bufs)
-      if (b.p) cudaFree(b.p);
     for (Ctx::Buf& b : c->batch_out)
       if (b.p) cudaFree(b.p);
     for (cudaEvent_t ev : c->ev)
@@ -999,6 +1091,29 @@ Status run_single_device(const double* d_pos, int64_t n, const double* cell9, co
   return Status{NLB_OK};
 }
 
+Status run_single_device(const double* d_pos, int64_t n, const double* cell9, const uint8_t* pbc,
+                         double cutoff, nlb_device_result* out, bool owned) {
+  Status st = run_single_device(d_pos, n, cell9, pbc, cutoff, out);
+  if (!st.ok() || !owned) return st;
+  // Hand the arrays (the context's result slots) over to the caller.
+  if (out->n_edges == 0) {
+    out->edge_index = nullptr;
+    out->shift = nullptr;
+    return st;
+  }
+  Ctx* c = nullptr;
+  st = get_ctx(&c);
+  if (!st.ok()) return st;
+  int64_t* ei = nullptr;
+  int32_t* sh = nullptr;
+  if (out->edge_index != c->bufs[kSlotOutEi].p || out->shift != c->bufs[kSlotOutSh].p)
+    return fail(NLB_ERR_CUDA, "device result is not in the context's result arrays");
+  take_result_arrays(*c, &ei, &sh);
+  out->edge_index = ei;
+  out->shift = sh;
+  return st;
+}
+
 }  // namespace nlb
 
 // ------------------------------------------------------------------ C ABI
@@ -1105,6 +1220,44 @@ int nlb_build_device(const double* d_positions, int64_t n_atoms, double cutoff,
   return run_single_device(d_positions, n_atoms, cell, pbc, cutoff, out).code;
 }
 
+int nlb_build_device_owned(const double* d_positions, int64_t n_atoms, double cutoff,
+                           const double* cell, const uint8_t* pbc, nlb_device_result* out) {
+  if (!out) return fail(NLB_ERR_VALUE, "out is NULL").code;
+  return run_single_device(d_positions, n_atoms, cell, pbc, cutoff, out, true).code;
+}
+
+int nlb_device_free(void* p, void* stream) {
+  if (!p) return NLB_OK;
+  ResultPool& rp = result_pool();
+  int dev = 0;
+  {
+    std::lock_guard<std::mutex> lk(rp.mu);
+    auto it = rp.owned.find(p);
+    if (it == rp.owned.end())
+      return fail(NLB_ERR_VALUE, "nlb_device_free: not a block from nlb_build_device_owned").code;
+    dev = it->second.first;
+    rp.owned.erase(it);
+    ++rp.returned;
+  }
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != dev) cudaSetDevice(dev);
+  cudaError_t e = cudaFreeAsync(p, static_cast<cudaStream_t>(stream));
+  if (prev != dev) cudaSetDevice(prev);
+  if (e != cudaSuccess) return cuda_fail(e, "nlb_device_free").code;
+  return NLB_OK;
+}
+
+void nlb_device_blocks(int64_t* out3) {
+  ResultPool& rp = result_pool();
+  std::lock_guard<std::mutex> lk(rp.mu);
+  int64_t bytes = 0;
+  for (auto& kv : rp.owned) bytes += (int64_t)kv.second.second;
+  out3[0] = rp.handed;
+  out3[1] = rp.returned;
+  out3[2] = bytes;
+}
+
 int nlb_copy_device(void* dst, const void* src, size_t bytes, void* stream) {
   if (bytes == 0) return NLB_OK;
   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice,
@@ -1116,6 +1269,8 @@ int nlb_copy_device(void* dst, const void* src, size_t bytes, void* stream) {
 void nlb_set_stream(void* stream) { tl_user_stream = static_cast<cudaStream_t>(stream); }
 
 int64_t nlb_kernel_launches(void) { return g_launches.load(); }
+
+int64_t nlb_graph_replays(void) { return g_graph_replays.load(); }
 
 int nlb_debug_scan_stall(int32_t tile, int32_t spin_limit) {
   if (tile < 0 || spin_limit < 1)

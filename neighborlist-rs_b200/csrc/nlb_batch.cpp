@@ -195,7 +195,297 @@ Status run_small(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts
   return Status{NLB_OK};
 }
 
+// ---------------------------------------------------------------- device-sized batches
+//
+// A batch whose systems all take the batched kernels, of a kind whose launch
+// shape is decided, runs plan -> count -> scan -> emit with no host round
+// trip in between: the emit pass reads each list's total from the device and
+// writes into grow-only arenas (capacity: the last batch's largest list x
+// 1.25, at least 16 edges per atom), writing nothing if a list does not fit
+// (the host then grows the arenas and emits again).  The second identical
+// call (same sizes, shape, cutoffs, buffers and stream) captures the
+// sequence as a CUDA graph and later calls replay it; the inputs are
+// uploaded before the graph runs, so new positions and cells of the same
+// shapes reuse it.
+
+struct BatchGraph {
+  std::vector<unsigned char> key;
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;
+  int64_t last_m = 0;  // largest list of the last device-sized batch
+};
+
+thread_local BatchGraph tl_bgraph[16];
+
+template <class T>
+void put(std::vector<unsigned char>& k, const T& v) {
+  const unsigned char* b = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), b, b + sizeof(T));
+}
+
+struct FastBatchArgs {
+  const double* d_pos;
+  const int64_t* d_starts;
+  const double* d_cells;
+  const uint8_t* d_pbcs;
+  const uint8_t* d_has;
+  int32_t n_sys;
+  int64_t row;
+  double rc_max;
+  bool disjoint, multi;
+  SysPlan* plans;
+  int32_t* flags;
+  uint32_t* counts;
+  int64_t* offs;
+  int64_t* scan_tmp;
+  int64_t* d_bounds;  // nullptr: no per-system offsets
+  BatchItems bw;
+  int64_t cap;
+};
+
+void issue_emit_fast(Ctx& c, const FastBatchArgs& a, const std::vector<double>& rc_sq,
+                     cudaStream_t s) {
+  const int32_t k = (int32_t)rc_sq.size();
+  for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
+    const CutoffSet cs = make_pass(rc_sq, g0, a.disjoint);
+    EmitTargets t;
+    std::memset(&t, 0, sizeof(t));
+    for (int32_t q = 0; q < cs.k; ++q) {
+      t.src[q] = static_cast<int64_t*>(c.batch_out[3 * (g0 + q)].p);
+      t.dst[q] = static_cast<int64_t*>(c.batch_out[3 * (g0 + q) + 1].p);
+      t.sh[q] = static_cast<int32_t*>(c.batch_out[3 * (g0 + q) + 2].p);
+    }
+    t.capacity = a.cap;
+    t.scan_error = a.scan_tmp + 1;
+    cudaMemsetAsync(a.flags + 1, 0, sizeof(int32_t) * 2, s);
+    launch_batch_emit(a.plans, a.bw, a.d_pos, cs, a.offs + (size_t)g0 * a.row, a.row, t,
+                      a.flags + 1, s);
+  }
+}
+
+void issue_batch_fast(Ctx& c, const FastBatchArgs& a, const std::vector<double>& rc_sq) {
+  cudaStream_t s = c.stream;
+  const int32_t k = (int32_t)rc_sq.size();
+  cudaMemsetAsync(a.flags, 0, sizeof(int32_t) * 3, s);
+  cudaMemsetAsync(a.counts, 0, sizeof(uint32_t) * (size_t)k * a.row, s);
+  launch_plan(a.d_pos, a.d_starts, 0, a.n_sys, a.d_cells, a.d_pbcs, a.d_has, a.rc_max,
+              g_bf_threshold.load(), a.multi ? 1 : 0, 0, a.plans, a.flags, s);
+  for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
+    const CutoffSet cs = make_pass(rc_sq, g0, a.disjoint);
+    cudaMemsetAsync(a.flags + 1, 0, sizeof(int32_t) * 2, s);
+    launch_batch_count(a.plans, a.bw, a.d_pos, cs, a.counts + (size_t)g0 * a.row, a.row,
+                       a.flags + 1, s);
+  }
+  exclusive_scan_u32(a.counts, (int64_t)k * a.row, a.offs, a.scan_tmp, s);
+  if (a.d_bounds)
+    for (int32_t q = 0; q < k; ++q)
+      launch_sys_bounds(a.plans, a.n_sys, a.offs + (size_t)q * a.row, a.row,
+                        a.d_bounds + (size_t)q * (a.n_sys + 1), s);
+  issue_emit_fast(c, a, rc_sq, s);
+}
+
+// Grows the k arenas (src, dst, shift per list) to `cap` edges each.
+bool arenas_for(Ctx& c, int32_t k, int64_t cap, cudaStream_t s) {
+  if (c.batch_out.size() < 3 * (size_t)k) c.batch_out.resize(3 * (size_t)k);
+  for (int32_t q = 0; q < k; ++q)
+    if (!grow_keep(c.batch_out[3 * q], 8 * (size_t)cap, 0, s) ||
+        !grow_keep(c.batch_out[3 * q + 1], 8 * (size_t)cap, 0, s) ||
+        !grow_keep(c.batch_out[3 * q + 2], 12 * (size_t)cap, 0, s))
+      return false;
+  return true;
+}
+
+int64_t arena_capacity(const Ctx& c, int32_t k) {
+  if (c.batch_out.size() < 3 * (size_t)k) return 0;
+  int64_t cap = INT64_MAX;
+  for (int32_t q = 0; q < k; ++q)
+    cap = std::min<int64_t>({cap, (int64_t)(c.batch_out[3 * q].cap / 8),
+                             (int64_t)(c.batch_out[3 * q + 1].cap / 8),
+                             (int64_t)(c.batch_out[3 * q + 2].cap / 12)});
+  return cap;
+}
+
+// The device-sized path for a batch of small systems only (one run).
+// *handled = false (nothing issued) when the batch's kind still has launch
+// shapes to time or phases are being profiled: the caller runs the counted
+// path instead.
+Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& starts,
+                      const int64_t* d_starts, const double* d_cells, const uint8_t* d_pbcs,
+                      const uint8_t* d_has, double rc_max, const std::vector<double>& rc_sq,
+                      const std::vector<int32_t>& order, bool disjoint, bool multi,
+                      nlb_result* outs, int64_t* sys_offsets, bool* handled) {
+  *handled = false;
+  if (c.prof) return Status{NLB_OK};
+  cudaStream_t s = c.stream;
+  const int32_t ns = (int32_t)starts.size() - 1;
+  const int32_t k = (int32_t)rc_sq.size();
+  const int64_t run_atoms = starts[ns];
+  std::vector<int64_t> sizes(ns);
+  for (int32_t i = 0; i < ns; ++i) sizes[i] = starts[i + 1] - starts[i];
+  ShapeTrials trials;
+  Status st = trials.prepare(c, make_tune_key(c.device, k, sizes.data(), ns, rc_max),
+                             sizes.data(), ns, kSlotBatch0 + 1);
+  if (!st.ok()) return st;
+  if (trials.timed) return Status{NLB_OK};
+  *handled = true;
+
+  FastBatchArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.d_pos = d_pos;
+  a.d_starts = d_starts;
+  a.d_cells = d_cells;
+  a.d_pbcs = d_pbcs;
+  a.d_has = d_has;
+  a.n_sys = ns;
+  a.row = run_atoms + 1;
+  a.rc_max = rc_max;
+  a.disjoint = disjoint;
+  a.multi = multi;
+  a.plans = slot<SysPlan>(c, kSlotBatch0 + 0, ns);
+  a.flags = slot<int32_t>(c, kSlotBatch0 + 2, 3);
+  a.counts = slot<uint32_t>(c, kSlotBatch0 + 3, (size_t)k * a.row);
+  a.offs = slot<int64_t>(c, kSlotBatch0 + 4, (size_t)k * a.row + 1);
+  a.scan_tmp = slot<int64_t>(c, kSlotBatch0 + 5, scan_tmp_elems((int64_t)k * a.row));
+  if (sys_offsets) a.d_bounds = slot<int64_t>(c, kSlotBatch0 + 11, (size_t)k * (ns + 1));
+  if (!a.plans || !a.flags || !a.counts || !a.offs || !a.scan_tmp ||
+      (sys_offsets && !a.d_bounds))
+    return fail(NLB_ERR_NOMEM, "device allocation failed");
+  a.bw = trials.w[0];
+
+  BatchGraph& bg = tl_bgraph[c.device & 15];
+  int64_t cap = std::max<int64_t>({4096, bg.last_m + bg.last_m / 4, 16 * run_atoms});
+  const int64_t have = arena_capacity(c, k);
+  if (have > cap) cap = have;
+  if (!arenas_for(c, k, cap, s)) return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
+  a.cap = cap;
+
+  // Everything the issued work depends on.
+  std::vector<unsigned char> key;
+  key.reserve(512 + 8 * (size_t)k);
+  put(key, a);
+  put(key, s);
+  put(key, g_bf_threshold.load());
+  for (int32_t q = 0; q < k; ++q) {
+    put(key, rc_sq[q]);
+    put(key, c.batch_out[3 * q].p);
+    put(key, c.batch_out[3 * q + 1].p);
+    put(key, c.batch_out[3 * q + 2].p);
+  }
+  const bool same = !scan_stall_armed() && key == bg.key;
+  bool launched = false;
+  if (same && bg.exec) {
+    if (cudaGraphLaunch(bg.exec, s) == cudaSuccess) {
+      note_launches(bg.launches);
+      note_graph_replay();
+      launched = true;
+    } else {
+      cudaGetLastError();
+    }
+  } else if (same && s != nullptr) {
+    // Second identical call: capture once, replay from now on.
+    if (bg.exec) {
+      cudaGraphExecDestroy(bg.exec);
+      bg.exec = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    const int64_t l0 = nlb_kernel_launches();
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      issue_batch_fast(c, a, rc_sq);
+      if (cudaStreamEndCapture(s, &graph) == cudaSuccess && graph) {
+        if (cudaGraphInstantiate(&bg.exec, graph, 0) != cudaSuccess) bg.exec = nullptr;
+        cudaGraphDestroy(graph);
+      }
+    }
+    cudaGetLastError();
+    bg.launches = (int)(nlb_kernel_launches() - l0);
+    if (bg.exec && cudaGraphLaunch(bg.exec, s) == cudaSuccess) {
+      note_graph_replay();
+      launched = true;
+    }
+    cudaGetLastError();
+  }
+  if (!launched) {
+    if (!same && bg.exec) {
+      cudaGraphExecDestroy(bg.exec);
+      bg.exec = nullptr;
+    }
+    issue_batch_fast(c, a, rc_sq);
+  }
+  bg.key.swap(key);
+
+  // One synchronisation: list totals, plan errors, the scan's error word,
+  // per-system offsets.
+  if (k + 3 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
+  cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), a.offs, sizeof(int64_t) * a.row,
+                                    sizeof(int64_t), (size_t)k + 1, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c.h_small + k + 1, a.flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c.h_small + k + 2, a.scan_tmp + 1, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, s);
+  std::vector<int64_t> bounds;
+  if (e == cudaSuccess && sys_offsets) {
+    bounds.resize((size_t)k * (ns + 1));
+    e = cudaMemcpyAsync(bounds.data(), a.d_bounds, sizeof(int64_t) * bounds.size(),
+                        cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "batched build");
+  if (c.h_small[k + 2] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+  const int32_t plan_err = (int32_t)(c.h_small[k + 1] & 0xffffffff);
+  if (plan_err == 1) return fail(NLB_ERR_VALUE, "Cell matrix is not invertible");
+  if (plan_err == 2) return fail(NLB_ERR_VALUE, "stencil too large for this cutoff and cell");
+  std::vector<int64_t> m(k);
+  int64_t m_max = 0;
+  for (int32_t q = 0; q < k; ++q) {
+    m[q] = c.h_small[q + 1] - c.h_small[q];
+    m_max = std::max(m_max, m[q]);
+  }
+  if (m_max > cap) {
+    // An arena was too small (nothing was written): grow and emit again.
+    a.cap = m_max + m_max / 8 + 1024;
+    if (!arenas_for(c, k, a.cap, s))
+      return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
+    issue_emit_fast(c, a, rc_sq, s);
+    bg.key.clear();  // arena pointers changed
+  }
+  bg.last_m = m_max;
+
+  // Exact-sized pinned results, in input cutoff order.
+  for (int32_t q = 0; q < k; ++q) {
+    nlb_result& r = outs[order[q]];
+    st = alloc_result(m[q], &r);
+    if (!st.ok()) return st;
+    if (m[q] == 0) continue;
+    cudaMemcpyAsync(r.edge_index, c.batch_out[3 * q].p, 8 * m[q], cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(r.edge_index + m[q], c.batch_out[3 * q + 1].p, 8 * m[q],
+                    cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(r.shift, c.batch_out[3 * q + 2].p, 12 * m[q], cudaMemcpyDeviceToHost, s);
+  }
+  if (sys_offsets) {
+    const size_t stride = (size_t)ns + 1;
+    for (int32_t q = 0; q < k; ++q) {
+      int64_t* row = sys_offsets + (size_t)order[q] * stride;
+      std::memcpy(row, bounds.data() + (size_t)q * stride, sizeof(int64_t) * stride);
+      row[ns] = m[q];
+    }
+  }
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    for (int32_t q = 0; q < k; ++q) nlb_result_free(&outs[order[q]]);
+    return cuda_fail(e, "batched emit");
+  }
+  return Status{NLB_OK};
+}
+
 }  // namespace
+
+void release_batch_graphs() {
+  for (BatchGraph& bg : tl_bgraph) {
+    if (bg.exec) cudaGraphExecDestroy(bg.exec);
+    bg = BatchGraph();
+  }
+}
 
 Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_batch,
                  const double* cutoffs, int32_t k, const double* cells, const uint8_t* pbcs,
@@ -259,6 +549,16 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
       cudaMemcpyAsync(d_has, has_cell, (size_t)n_sys, cudaMemcpyHostToDevice, s);
     else
       cudaMemsetAsync(d_has, 1, (size_t)n_sys, s);
+  }
+
+  bool all_small = true;
+  for (int32_t i = 0; i < n_sys && all_small; ++i)
+    all_small = starts[i + 1] - starts[i] <= kBatchMaxAtoms;
+  if (all_small) {
+    bool handled = false;
+    st = run_small_fast(*c, d_pos, starts, d_starts, d_cells, d_pbcs, d_has, rc_max, rc_sq, order,
+                        disjoint, multi, outs, sys_offsets, &handled);
+    if (!st.ok() || handled) return st;
   }
 
   Outputs out(*c, k);

@@ -208,6 +208,7 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
   if (same && fs.exec) {
     if (cudaGraphLaunch(fs.exec, c.stream) == cudaSuccess) {
       note_launches(fs.launches);
+      note_graph_replay();
       launched = true;
     } else {
       cudaGetLastError();
@@ -231,7 +232,10 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
     }
     cudaGetLastError();
     fs.launches = (int)(nlb_kernel_launches() - l0);
-    if (fs.exec && cudaGraphLaunch(fs.exec, c.stream) == cudaSuccess) launched = true;
+    if (fs.exec && cudaGraphLaunch(fs.exec, c.stream) == cudaSuccess) {
+      note_graph_replay();
+      launched = true;
+    }
     cudaGetLastError();
   }
   if (!launched) {

@@ -72,6 +72,7 @@ struct Ctx {
   struct Buf {
     void* p = nullptr;
     size_t cap = 0;
+    bool pooled = false;  // from the result pool (stream-ordered), not cudaMalloc
   };
   int device = 0;
   cudaStream_t own_stream = nullptr;
@@ -106,10 +107,18 @@ struct Ctx {
 };
 
 Status get_ctx(Ctx** out);
+// Hands the context's single-system result arrays (slots kSlotOutEi and
+// kSlotOutSh, allocated from the per-device result pool) over to the caller:
+// the context forgets them and its next build allocates fresh ones from the
+// pool.  The caller returns each with nlb_device_free.
+void take_result_arrays(Ctx& c, int64_t** ei, int32_t** sh);
 // Frees the calling thread's contexts and fast-path graphs (threads that end
 // before the process does, e.g. server workers).
 void release_thread_ctx();
 void release_fast_states();
+void release_batch_graphs();
+// Counts CUDA-graph replays of the fast paths (nlb_graph_replays).
+void note_graph_replay();
 bool fp32_search_enabled();
 
 template <class T>

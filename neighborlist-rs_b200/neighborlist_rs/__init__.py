@@ -548,15 +548,56 @@ def build_device_raw(cell, positions_ptr: int, n_atoms: int, cutoff: float):
     return int(r.n_edges), r.edge_index, r.shift
 
 
+_lib.nlb_build_device_owned.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, _dp,
+                                       _u8p, ctypes.POINTER(_DevResult)]
+_lib.nlb_device_free.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+_lib.nlb_device_blocks.argtypes = [ctypes.POINTER(ctypes.c_int64)]
+
+
+class _DeviceBlock:
+    """Owner of one device block handed over by nlb_build_device_owned,
+    exposed through the CUDA array interface (version 3) so that torch (and
+    CuPy, Numba, ...) view it without a copy; the block goes back to the
+    library's pool (nlb_device_free, ordered on the producing stream) when
+    the last view is gone."""
+
+    __slots__ = ("ptr", "stream", "__cuda_array_interface__", "__weakref__")
+
+    def __init__(self, ptr: int, shape, typestr: str, stream: int):
+        self.ptr = ptr
+        self.stream = stream
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3, "strides": None,
+                                         "stream": None}
+
+    def __del__(self):
+        if self.ptr:
+            _lib.nlb_device_free(ctypes.c_void_p(self.ptr), ctypes.c_void_p(self.stream))
+            self.ptr = 0
+
+
+def device_blocks() -> dict:
+    """Counters of the zero-copy device result blocks: handed out, returned,
+    and bytes still outstanding."""
+    buf = (ctypes.c_int64 * 3)()
+    _lib.nlb_device_blocks(buf)
+    return {"handed": int(buf[0]), "returned": int(buf[1]), "outstanding_bytes": int(buf[2])}
+
+
 def build_neighborlists_torch(cell, positions, cutoff, directed=False, vectors=False,
                               distances=False):
     """GPU-resident variant of build_neighborlists for torch pipelines:
     ``positions`` is a CUDA float64 tensor (N, 3); returns
     {"edge_index": int64 (2, M), "shift": int32 (M, 3)} as CUDA tensors on the
-    same device, produced on the current torch stream (no host round trip
-    for the edge arrays).  directed / vectors / distances as in
-    build_neighborlists_ex (adds "vectors" float64 (M, 3) and "distances"
-    float64 (M,))."""
+    same device, produced on the current torch stream.  The tensors are the
+    library's result blocks themselves (zero-copy: the build writes them in
+    place and hands them over; they return to the library's pool when the
+    tensors are freed, ordered on the stream that was current for the build,
+    so a consumer on another stream keeps them alive until its work there is
+    done, as with torch's own record_stream rule).  directed / vectors /
+    distances as in build_neighborlists_ex (adds "vectors" float64 (M, 3) and
+    "distances" float64 (M,); those results are copied out of the library's
+    workspace)."""
     if directed or vectors or distances:
         return _torch_ex(cell, positions, cutoff, directed, vectors, distances)
     import torch
@@ -573,18 +614,25 @@ def build_neighborlists_torch(cell, positions, cutoff, directed=False, vectors=F
         _check_cutoff(cutoff)
         return {"edge_index": torch.zeros((2, 0), dtype=torch.int64, device=dev),
                 "shift": torch.zeros((0, 3), dtype=torch.int32, device=dev)}
+    c = _check_cutoff(cutoff)
+    h, pb = _cell_args(cell)
     with torch.cuda.device(dev):
         stream = torch.cuda.current_stream(dev)
         set_stream(stream.cuda_stream)
         try:
-            m, ei_ptr, sh_ptr = build_device_raw(cell, pos.data_ptr(), n, cutoff)
-            ei = torch.empty((2, m), dtype=torch.int64, device=dev)
-            sh = torch.empty((m, 3), dtype=torch.int32, device=dev)
-            if m:
-                _cudart_copy(ei.data_ptr(), ei_ptr, 16 * m, stream.cuda_stream)
-                _cudart_copy(sh.data_ptr(), sh_ptr, 12 * m, stream.cuda_stream)
+            r = _DevResult()
+            _check(_lib.nlb_build_device_owned(ctypes.c_void_p(pos.data_ptr()), n, c, h, pb,
+                                               ctypes.byref(r)))
         finally:
             set_stream(None)
+        m = int(r.n_edges)
+        if m == 0:
+            return {"edge_index": torch.zeros((2, 0), dtype=torch.int64, device=dev),
+                    "shift": torch.zeros((0, 3), dtype=torch.int32, device=dev)}
+        ei = torch.as_tensor(_DeviceBlock(r.edge_index, (2, m), "<i8", stream.cuda_stream),
+                             device=dev)
+        sh = torch.as_tensor(_DeviceBlock(r.shift, (m, 3), "<i4", stream.cuda_stream),
+                             device=dev)
     return {"edge_index": ei, "shift": sh}
 
 
