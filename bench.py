@@ -680,15 +680,18 @@ def verlet_measurements(nl, torch):
             "rebuilds": st["rebuilds"], "updates": st["updates"]}
 
 
-def run_stream(srv, reqs, rate, seed=0):
+def run_stream(srv, reqs, rate, seed=0, device=False):
     """Offers `reqs` [(cell, positions, cutoff)] to the server through its
-    Python API (Server.submit / wait, numpy results): Poisson arrivals at
+    Python API (Server.submit / wait, numpy results; device=True: results
+    stay in HBM and are released right after the wait): Poisson arrivals at
     `rate` req/s (None: all at once).  One client thread submits each
     request when it is due and, in between, collects finished results in
     arrival order (results dropped).  Latency is the server's submit -> done
-    time of each request."""
+    time of each request; the admission wait is the mean submit -> taken-by-
+    a-worker time, from the server's counters."""
     import collections
 
+    st0 = srv.stats()
     n = len(reqs)
     arrivals = (np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, n))
                 if rate else np.zeros(n))
@@ -701,7 +704,7 @@ def run_stream(srv, reqs, rate, seed=0):
         now = time.perf_counter() - t0
         if i < n and arrivals[i] <= now:
             c, p, rc = reqs[i]
-            pending.append((i, srv.submit(c, p, rc)))
+            pending.append((i, srv.submit(c, p, rc, device_result=device)))
             i += 1
             if i == n:
                 t_sub = time.perf_counter() - t0
@@ -716,13 +719,21 @@ def run_stream(srv, reqs, rate, seed=0):
             continue
         pending.popleft()
         lat[j] = ms
-        edges[j] = r["edge_index"].shape[1]
+        if device:
+            edges[j] = r.n_edges
+            r.release()
+        else:
+            edges[j] = r["edge_index"].shape[1]
         del r
     t = time.perf_counter() - t0
+    st1 = srv.stats()
+    started = max(1, (st1["completed"] + st1["failed"]) - (st0["completed"] + st0["failed"]))
     return {"offered_req_per_s": rate, "submitted_req_per_s": n / t_sub,
             "systems_per_s": n / t, "edges_per_s": float(edges.sum()) / t,
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "requests": n, "edges": int(edges.sum())}
+            "mean_admission_wait_ms": 1e-3 * (st1["us_queue_wait"] - st0["us_queue_wait"]) / started,
+            "max_queued": st1["max_queued"], "requests": n, "edges": int(edges.sum()),
+            "results": "device" if device else "host"}
 
 
 def run_stream_raw(srv, reqs, device=False):
@@ -786,26 +797,45 @@ def served_measurements(nl):
         return {"systems_per_s": len(reqs) / t, "edges_per_s": m / t, "requests": len(reqs)}
 
     out = {}
-    small = as_reqs(W.request_stream(4096, seed=21, n_range=(16, 2048)))
+    small = as_reqs(W.request_stream(8192, seed=21, n_range=(16, 2048)))
     plain(small[:1024])
     res = {"plain_per_request_loop": plain(small[:1024])}
     with Server(hbm_budget_bytes=40 << 30, workers=4, max_batch=4096) as srv:
         # Untimed: the first runs pin host blocks and decide the batch kinds.
-        run_stream(srv, small, None)
-        run_stream_raw(srv, small)
-        res["saturated_python_api"] = run_stream(srv, small, None)
-        res["saturated_c_abi"] = run_stream_raw(srv, small)
-        run_stream_raw(srv, small, device=True)
-        res["saturated_c_abi_device_results"] = run_stream_raw(srv, small, device=True)
+        run_stream(srv, small[:4096], None)
+        run_stream_raw(srv, small[:4096])
+        res["saturated_python_api"] = run_stream(srv, small[:4096], None)
+        res["saturated_c_abi"] = run_stream_raw(srv, small[:4096])
+        run_stream_raw(srv, small[:4096], device=True)
+        res["saturated_c_abi_device_results"] = run_stream_raw(srv, small[:4096], device=True)
+        # Poisson offered loads: at least 5000 requests per rate (8192 from
+        # 10k req/s up), so that each p99 rests on 50+ samples.
         for rate in (1000, 2000, 10000, 25000, 50000):
-            k = min(len(small), max(512, int(rate * 0.4)))
+            k = 5000 if rate < 10000 else len(small)
             res[f"poisson_{rate}"] = run_stream(srv, small[:k], rate, seed=rate)
         st = srv.stats()
         res["batches"] = st["batches"]
         res["largest_batch"] = st["largest_batch"]
-    out["small_mix_4096"] = dict(
-        res, workload="4096 requests, N log-uniform [16, 2048], 70% orthorhombic / 20% "
+    out["small_mix"] = dict(
+        res, workload="8192 requests, N log-uniform [16, 2048], 70% orthorhombic / 20% "
                       "triclinic / 10% isolated, rho 0.1, rc in {5, 6, 8}")
+    # The served distribution itself (N log-uniform [16, 1e6]) under Poisson
+    # load: device-resident results (HBM-bound) and host results (bound by
+    # the ~50 GB/s host link: ~2.5 MB of results per request on average).
+    full_dist = as_reqs(W.request_stream(600, seed=23))
+    res = {}
+    with Server(hbm_budget_bytes=40 << 30, workers=4, max_batch=4096) as srv:
+        run_stream_raw(srv, full_dist[:200], device=True)
+        run_stream(srv, full_dist[:200], None, device=True)
+        for rate in (500, 1000, 2000):
+            res[f"poisson_{rate}_device"] = run_stream(srv, full_dist, rate, seed=rate, device=True)
+        run_stream(srv, full_dist[:100], None)
+        for rate in (100, 200):
+            res[f"poisson_{rate}_host"] = run_stream(srv, full_dist[:400], rate, seed=rate)
+    out["full_distribution_poisson"] = dict(
+        res, workload="600 requests of the served distribution (N log-uniform [16, 1e6], "
+                      "70% orthorhombic / 20% triclinic / 10% isolated, rho 0.1, rc in {5, 6, 8}); "
+                      "host-result rates use the first 400")
     full = as_reqs(W.request_stream(48, seed=22))
     plain(full)
     res = {"plain_per_request_loop": plain(full)}

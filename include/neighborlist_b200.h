@@ -318,11 +318,13 @@ int nlb_build_noalloc(const double* d_positions, int64_t n_atoms, double cutoff,
  *   the ticket is retired; device results stay owned by the server until
  *   nlb_server_release, which the caller issues once its own work reading
  *   them has completed.
- * nlb_server_stats: fills 14 counters: submitted, completed, failed, batches,
+ * nlb_server_stats: fills 16 counters: submitted, completed, failed, batches,
  *   HBM bytes reserved, queued requests, largest batch, budget, then worker
  *   wall time in microseconds (all workers) spent in: batch staging and
  *   launches, waiting for the count pass, issuing result copies, waiting
- *   for the emit pass and copies, large requests; then cancelled requests.
+ *   for the emit pass and copies, large requests; then cancelled requests,
+ *   the summed admission wait of started requests (submit -> taken by a
+ *   worker, microseconds) and the deepest queue seen.
  * nlb_server_pause: paused != 0 stops the workers from taking new work
  *   (requests queue up, running work finishes); 0 resumes.
  * nlb_server_cancel: withdraws a queued request (it never runs) or frees a

@@ -20,6 +20,7 @@
 // scan gives every system's global edge offsets, so the emit pass writes the
 // concatenated, exact-sized output (systems in input order) directly.
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "k_traverse.cuh"
@@ -362,6 +363,7 @@ __device__ __forceinline__ void visit_smem_grid_atom(const SysPlan& P, const Sme
       cshift[2] = __shfl_sync(0xffffffffu, sh[2], src);
       const bool shifted = (cshift[0] | cshift[1] | cshift[2]) != 0;
       for (int jb = j0; jb < j1; jb += 32) {
+        sink.at(jb, cshift);
         const int j = jb + lane;
         bool hit = false;
         double d2 = 0.0;
@@ -391,7 +393,9 @@ __device__ __forceinline__ void visit_smem_brute_atom(const SysPlan& P, const Sm
   const int lane = threadIdx.x & 31;
   const int n = P.n;
   const double xi = v.px[i], yi = v.py[i], zi = v.pz[i];
+  const int32_t no_shift[3] = {0, 0, 0};
   for (int jb = i + 1; jb < n; jb += 32) {
+    sink.at(jb, no_shift);
     const int j = jb + lane;
     bool hit = false;
     double d2 = 0.0;
@@ -450,14 +454,80 @@ __device__ __forceinline__ void system_cutoff(const CutoffSet& cs, const SysPlan
   out.disjoint = 0;
 }
 
-template <int THREADS>
+// Record sink of the single-cutoff count pass: besides the count, every
+// candidate step of the atom with at least one hit becomes a record {hit
+// mask, first candidate, the cell's image shift in three signed 10-bit
+// fields}.  Lane l buffers the atom's l-th pending record; 32 pending
+// records (and the atom's last ones) are flushed as one segment whose header
+// holds the atom's run slot, its edges in earlier segments, the record count
+// and the system.  A segment or a shift that does not fit sets the overflow
+// flag: the emit pass then recomputes instead of expanding.
+struct RecSink {
+  const CutoffSet* cs;
+  BatchRecords rb;
+  uint32_t cnt = 0;  // lane 0: the atom's edge count
+  uint32_t r_mask = 0, r_j = 0, r_sh = 0;  // lane l: pending record l
+  int n_rec = 0, e_done = 0, e_buf = 0;  // warp-uniform
+  int32_t p_abs = 0, sys = 0;
+  uint32_t cur_j = 0, cur_sh = 0;
+  bool sh_ok = true;
+
+  __device__ __forceinline__ void at(int32_t jb, const int32_t* csh) {
+    cur_j = (uint32_t)jb;
+    sh_ok = csh[0] >= -511 && csh[0] <= 511 && csh[1] >= -511 && csh[1] <= 511 &&
+            csh[2] >= -511 && csh[2] <= 511;
+    cur_sh = ((uint32_t)csh[0] & 1023u) | (((uint32_t)csh[1] & 1023u) << 10) |
+             (((uint32_t)csh[2] & 1023u) << 20);
+  }
+  __device__ __forceinline__ void flush() {
+    if (n_rec == 0) return;
+    const int lane = threadIdx.x & 31;
+    int sg = 0;
+    if (lane == 0) sg = atomicAdd(rb.seg_top, 1);
+    sg = __shfl_sync(0xffffffffu, sg, 0);
+    if (sg < rb.seg_cap) {
+      if (lane < n_rec) {
+        uint32_t* r = rb.rec + ((size_t)sg * 32 + lane) * 3;
+        r[0] = r_mask;
+        r[1] = r_j;
+        r[2] = r_sh;
+      }
+      if (lane == 0) rb.seg_hdr[sg] = make_int4(p_abs, e_done, n_rec, sys);
+    } else if (lane == 0) {
+      *rb.overflow = 1;
+    }
+    e_done += e_buf;
+    e_buf = 0;
+    n_rec = 0;
+  }
+  __device__ __forceinline__ void operator()(bool hit, double d2, int32_t, int32_t,
+                                             const int32_t*) {
+    const int lane = threadIdx.x & 31;
+    const bool h = hit && d2 < cs->rc_sq[0] && !(cs->disjoint && d2 < cs->lower_sq);
+    const unsigned m = __ballot_sync(0xffffffffu, h);
+    if (!m) return;
+    if (lane == 0) cnt += __popc(m);
+    if (!sh_ok && lane == 0) *rb.overflow = 1;
+    if (lane == n_rec) {
+      r_mask = m;
+      r_j = cur_j;
+      r_sh = cur_sh;
+    }
+    ++n_rec;
+    e_buf += __popc(m);
+    if (n_rec == 32) flush();
+  }
+};
+
+template <int THREADS, bool REC>
 // 80 registers per thread for 64 / 128 / 256-thread CTAs.  The 512-thread count
 // spills at the 64-register budget of two CTAs per SM; one CTA per SM with
 // room for ~106 registers measured 7-8 % faster.
 __global__ void __launch_bounds__(THREADS, THREADS >= 512 ? 1 : 768 / THREADS)
     k_batch_count(const SysPlan* __restrict__ plans, const int2* __restrict__ items, int n_items,
                   int chunk, const double* __restrict__ pos, int cap, CutoffSet cs,
-                  uint32_t* __restrict__ counts, int64_t row, int* __restrict__ work) {
+                  uint32_t* __restrict__ counts, int64_t row, int* __restrict__ work,
+                  BatchRecords rb) {
   constexpr int kWarps = THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ SysPlan P;
@@ -477,13 +547,34 @@ __global__ void __launch_bounds__(THREADS, THREADS >= 512 ? 1 : 768 / THREADS)
     }
     load_system(P, pos, v);
     const int p_end = min(P.n, item.y + chunk);
+    if (REC) {
+      // The sorted meta of this item's atoms (brute force: unsorted, no
+      // wrap shifts) for the expansion pass.
+      for (int p = item.y + threadIdx.x; p < p_end; p += blockDim.x) {
+        SlotMeta m{0, 0, 0, p};
+        if (P.method == 2) m = v.meta[p];
+        rb.meta[P.slot + p] = m;
+      }
+    }
     for (int p = item.y + warp; p < p_end; p += kWarps) {
-      CountSink sink{csp, 0u};
-      if (P.method == 2)
-        visit_smem_grid_atom(P, v, p, csp->max_sq, sink);
-      else
-        visit_smem_brute_atom(P, v, p, csp->max_sq, sink);
-      if (lane < csp->k) counts[(int64_t)lane * row + P.slot + p] = sink.cnt;
+      if (REC) {
+        RecSink sink{csp, rb};
+        sink.p_abs = P.slot + p;
+        sink.sys = item.x;
+        if (P.method == 2)
+          visit_smem_grid_atom(P, v, p, csp->max_sq, sink);
+        else
+          visit_smem_brute_atom(P, v, p, csp->max_sq, sink);
+        sink.flush();
+        if (lane == 0) counts[P.slot + p] = sink.cnt;
+      } else {
+        CountSink sink{csp, 0u};
+        if (P.method == 2)
+          visit_smem_grid_atom(P, v, p, csp->max_sq, sink);
+        else
+          visit_smem_brute_atom(P, v, p, csp->max_sq, sink);
+        if (lane < csp->k) counts[(int64_t)lane * row + P.slot + p] = sink.cnt;
+      }
     }
     __syncthreads();
   }
@@ -568,6 +659,89 @@ __global__ void k_sys_bounds(const SysPlan* __restrict__ plans, int n_sys,
   if (s == n_sys) out[s] = offs[row - 1] - offs[0];
 }
 
+// Expansion of the count pass's records into the single-cutoff list: one
+// warp per segment; each record's hit lanes write (i, j, shift) at the
+// atom's next slots, in record order -- the order the recomputing emit pass
+// writes.  Shifts: (s_j - s_i) + the cell's image shift (cell list; zero
+// wrap shifts and image for raw brute force); the minimum-image systems
+// recompute the pair's shift from the raw positions exactly as the count
+// pass did.
+__global__ void __launch_bounds__(256)
+    k_batch_expand(BatchRecords rb, const SysPlan* __restrict__ plans,
+                   const double* __restrict__ pos, const int64_t* __restrict__ offs, int64_t row,
+                   EmitTargets t) {
+  if (t.scan_error && *t.scan_error != 0) return;
+  if (t.capacity > 0 && offs[row] - offs[0] > t.capacity) return;
+  if (*rb.overflow) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *rb.need_recompute = 1;
+    return;
+  }
+  const int n_seg = min(*rb.seg_top, rb.seg_cap);
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int sg = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); sg < n_seg; sg += warps) {
+    const int4 hdr = rb.seg_hdr[sg];
+    const SysPlan* P = plans + hdr.w;
+    const int32_t method = P->method;
+    const int64_t start = P->start;
+    const int32_t slot = P->slot;
+    const SlotMeta mi = rb.meta[hdr.x];
+    uint32_t my_mask = 0, my_j = 0, my_sh = 0;
+    if (lane < hdr.z) {
+      const uint32_t* r = rb.rec + ((size_t)sg * 32 + lane) * 3;
+      my_mask = r[0];
+      my_j = r[1];
+      my_sh = r[2];
+    }
+    int64_t cur = t.base[0] + (offs[hdr.x] - offs[0]) + hdr.y;
+    const int64_t idx_off = t.local_indices ? t.index_offset : start + t.index_offset;
+    int64_t* src = t.src[0];
+    int64_t* dst = t.dst[0];
+    if (t.system_blocks) {
+      // This system's list is one [src | dst] block at src[0] + 2 b0.
+      const int64_t b0 = offs[slot] - offs[0];
+      const int64_t m_sys = offs[slot + P->n] - offs[slot];
+      src = t.src[0] + b0;
+      dst = t.src[0] + b0 + m_sys;
+    }
+    double xi = 0.0, yi = 0.0, zi = 0.0;
+    if (method == 1) {
+      const double* pi = pos + 3 * (start + mi.orig);
+      xi = pi[0];
+      yi = pi[1];
+      zi = pi[2];
+    }
+    for (int r = 0; r < hdr.z; ++r) {
+      const uint32_t mask = __shfl_sync(0xffffffffu, my_mask, r);
+      const int32_t j0 = (int32_t)__shfl_sync(0xffffffffu, my_j, r);
+      const uint32_t psh = __shfl_sync(0xffffffffu, my_sh, r);
+      if ((mask >> lane) & 1u) {
+        const SlotMeta mj = rb.meta[slot + j0 + lane];
+        int32_t s[3];
+        if (method == 1) {
+          const double* pj = pos + 3 * (start + mj.orig);
+          double df[3];
+          matvec(P->g.hinv, dsub(pj[0], xi), dsub(pj[1], yi), dsub(pj[2], zi), df);
+#pragma unroll
+          for (int a = 0; a < 3; ++a) s[a] = sat_i32(P->pbc[a] ? -round(df[a]) : 0.0);
+        } else {
+          s[0] = (mj.sx - mi.sx) + ((int32_t)(psh << 22) >> 22);
+          s[1] = (mj.sy - mi.sy) + ((int32_t)(psh << 12) >> 22);
+          s[2] = (mj.sz - mi.sz) + ((int32_t)(psh << 2) >> 22);
+        }
+        const int64_t e = cur + __popc(mask & lanemask_lt());
+        src[e] = (int64_t)mi.orig + idx_off;
+        dst[e] = (int64_t)mj.orig + idx_off;
+        int32_t* sp = t.sh[0] + 3 * e;
+        sp[0] = s[0];
+        sp[1] = s[1];
+        sp[2] = s[2];
+      }
+      cur += __popc(mask);
+    }
+  }
+}
+
 int grid_for(const void* func, int threads, size_t smem) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
@@ -615,14 +789,19 @@ const BatchShape kBatchShapeTable[kBatchShapes] = {
 
 namespace {
 
-using CountFn = decltype(&k_batch_count<256>);
+using CountFn = decltype(&k_batch_count<256, false>);
 using EmitFn = decltype(&k_batch_emit<256>);
 
-CountFn count_fn(int threads) {
-  return threads <= 64    ? &k_batch_count<64>
-         : threads <= 128 ? &k_batch_count<128>
-         : threads <= 256 ? &k_batch_count<256>
-                          : &k_batch_count<512>;
+CountFn count_fn(int threads, bool rec = false) {
+  if (rec)
+    return threads <= 64    ? &k_batch_count<64, true>
+           : threads <= 128 ? &k_batch_count<128, true>
+           : threads <= 256 ? &k_batch_count<256, true>
+                            : &k_batch_count<512, true>;
+  return threads <= 64    ? &k_batch_count<64, false>
+         : threads <= 128 ? &k_batch_count<128, false>
+         : threads <= 256 ? &k_batch_count<256, false>
+                          : &k_batch_count<512, false>;
 }
 EmitFn emit_fn(int threads) {
   return threads <= 64    ? &k_batch_emit<64>
@@ -639,6 +818,7 @@ void preload_batch_kernels() {
   cudaFuncAttributes a;
   for (int threads : {64, 128, 256, 512}) {
     cudaFuncGetAttributes(&a, (const void*)count_fn(threads));
+    cudaFuncGetAttributes(&a, (const void*)count_fn(threads, true));
     cudaFuncGetAttributes(&a, (const void*)emit_fn(threads));
   }
   cudaGetLastError();
@@ -646,26 +826,36 @@ void preload_batch_kernels() {
 
 void launch_batch_count(const SysPlan* plans, const BatchItems& w, const double* pos,
                         const CutoffSet& cs, uint32_t* counts, int64_t row, int* work2,
-                        cudaStream_t s) {
+                        cudaStream_t s, const BatchRecords* rec) {
   const BatchShape& sh = w.shape;
+  BatchRecords rb;
+  std::memset(&rb, 0, sizeof(rb));
+  if (rec) rb = *rec;
   if (w.n_large > 0) {
     const size_t smem = batch_smem_bytes(w.cap_large);
-    const CountFn k = count_fn(sh.large_threads);
+    const CountFn k = count_fn(sh.large_threads, rec != nullptr);
     ensure_smem_attr((const void*)k, (int)smem);
     const int grid = std::min(grid_for((const void*)k, sh.large_threads, smem), w.n_large);
     k<<<grid, sh.large_threads, smem, s>>>(plans, w.items, w.n_large, sh.chunk, pos,
-                                           w.cap_large, cs, counts, row, work2);
+                                           w.cap_large, cs, counts, row, work2, rb);
     note_launches(1);
   }
   if (w.n_small > 0) {
     const size_t smem = batch_smem_bytes(w.cap_small);
-    const CountFn k = count_fn(sh.small_threads);
+    const CountFn k = count_fn(sh.small_threads, rec != nullptr);
     ensure_smem_attr((const void*)k, (int)smem);
     const int grid = std::min(grid_for((const void*)k, sh.small_threads, smem), w.n_small);
     k<<<grid, sh.small_threads, smem, s>>>(plans, w.items + w.n_large, w.n_small, 1 << 30, pos,
-                                           w.cap_small, cs, counts, row, work2 + 1);
+                                           w.cap_small, cs, counts, row, work2 + 1, rb);
     note_launches(1);
   }
+}
+
+void launch_batch_expand(const BatchRecords& rb, const SysPlan* plans, const double* pos,
+                         const int64_t* offs, int64_t row, const EmitTargets& t, cudaStream_t s) {
+  const int grid = grid_for((const void*)k_batch_expand, 256, 0);
+  k_batch_expand<<<grid, 256, 0, s>>>(rb, plans, pos, offs, row, t);
+  note_launches(1);
 }
 
 void launch_batch_emit(const SysPlan* plans, const BatchItems& w, const double* pos,

@@ -178,7 +178,8 @@ __global__ void __launch_bounds__(kSortThreads)
               double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz,
               SlotMeta* __restrict__ meta, float4* __restrict__ p32, int32_t* __restrict__ sbin,
               GroupRec* __restrict__ groups, int32_t* __restrict__ irr_list,
-              uint8_t* __restrict__ irr, int32_t* __restrict__ counters) {
+              uint8_t* __restrict__ irr, int32_t* __restrict__ counters,
+              float4* __restrict__ cbox) {
   __shared__ uint64_t sk[kSortCap];
   __shared__ int32_t sv[kSortCap];
   pdl_wait();
@@ -286,6 +287,29 @@ __global__ void __launch_bounds__(kSortThreads)
       if (!same) irr_list[atomicAdd(&counters[1], 1)] = (int32_t)p;
     }
   }
+  if (p32 && cbox) {
+    // Bounding box of each 32-atom chunk (the p32 values just written by this
+    // block's threads).
+    __syncthreads();
+    const int ng = (int)((cnt + 31) / 32);
+    for (int k = threadIdx.x; k < ng; k += blockDim.x) {
+      const int64_t c0 = s + 32 * (int64_t)k;
+      const int64_t c1 = c0 + 32 < e ? c0 + 32 : e;
+      float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+      float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+      for (int64_t p = c0; p < c1; ++p) {
+        const float4 a = p32[p];
+        lo.x = fminf(lo.x, a.x);
+        lo.y = fminf(lo.y, a.y);
+        lo.z = fminf(lo.z, a.z);
+        hi.x = fmaxf(hi.x, a.x);
+        hi.y = fmaxf(hi.y, a.y);
+        hi.z = fmaxf(hi.z, a.z);
+      }
+      cbox[2 * c0] = lo;
+      cbox[2 * c0 + 1] = hi;
+    }
+  }
   if (p32 && threadIdx.x == 0) {
     const int ng = (int)((cnt + 31) / 32);
     const int base = atomicAdd(&counters[0], ng);
@@ -367,7 +391,7 @@ void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const 
              b.bin_start, b.bin_fill, b.skey, b.sidx);
   launch_pdl(k_binsort, dim3((unsigned)g.total_bins), dim3(kSortThreads), 0, s, g, pos,
              b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta, b.p32,
-             b.sbin, b.groups, b.irr_list, b.irr, b.counters);
+             b.sbin, b.groups, b.irr_list, b.irr, b.counters, b.cbox);
   note_launches(3);
 }
 

@@ -435,9 +435,22 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? (K == 1 ? 3 : 1) : (K 
     if (work) {
       const float4 a = b.p32[p];
       const int32_t io = __float_as_int(a.w);
-      const float ux = __double2float_rn(dsub(cs[0], cb[0])) - a.x;
-      const float uy = __double2float_rn(dsub(cs[1], cb[1])) - a.y;
-      const float uz = __double2float_rn(dsub(cs[2], cb[2])) - a.z;
+      const float tx = __double2float_rn(dsub(cs[0], cb[0]));
+      const float ty = __double2float_rn(dsub(cs[1], cb[1]));
+      const float tz = __double2float_rn(dsub(cs[2], cb[2]));
+      const float ux = tx - a.x;
+      const float uy = ty - a.y;
+      const float uz = tz - a.z;
+      // Chunk pruning (count pass, dense grids): the group's box in its bin
+      // frame; a candidate chunk whose box, moved by the cell translation,
+      // stays farther than the band allows is skipped (its masks are zero).
+      const bool prune = !EMIT && b.cbox != nullptr;
+      float4 glo = make_float4(0.f, 0.f, 0.f, 0.f), ghi = glo;
+      if (prune) {
+        glo = b.cbox[2 * (int64_t)grp.first];
+        ghi = b.cbox[2 * (int64_t)grp.first + 1];
+      }
+      const float skip_sq = hi[K - 1] + (hi[K - 1] - lo[K - 1]);
       const float2 ux2 = make_float2(ux, ux), uy2 = make_float2(uy, uy), uz2 = make_float2(uz, uz);
       const bool shifted = (sh[0] | sh[1] | sh[2]) != 0;
       // Half-list predicate io < jo || (io == jo && shifted) as one compare.
@@ -446,6 +459,20 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? (K == 1 ? 3 : 1) : (K 
       if (EMIT) mi = b.meta[p];
       for (int32_t jb = b0; jb < b1; jb += 32) {
         const int32_t nj = b1 - jb < 32 ? b1 - jb : 32;
+        if (prune) {
+          const float4 clo = b.cbox[2 * (int64_t)jb], chi = b.cbox[2 * (int64_t)jb + 1];
+          const float gx = fmaxf(fmaxf((clo.x + tx) - ghi.x, glo.x - (chi.x + tx)), 0.f);
+          const float gy = fmaxf(fmaxf((clo.y + ty) - ghi.y, glo.y - (chi.y + ty)), 0.f);
+          const float gz = fmaxf(fmaxf((clo.z + tz) - ghi.z, glo.z - (chi.z + tz)), 0.f);
+          if (gx * gx + gy * gy + gz * gz > skip_sq) {
+            if (mbase >= 0) {
+#pragma unroll
+              for (int q = 0; q < K; ++q)
+                b.masks[(int64_t)mbase + (int64_t)q * words + (jb - b0) + lane] = 0u;
+            }
+            continue;
+          }
+        }
         // Stage 32 candidates; slots past the bin end hold a far sentinel.
         float4 qv = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
         if (lane < nj) {

@@ -23,9 +23,12 @@ __device__ __forceinline__ double shfl_d(double v, int src) {
 }
 
 // Hit sink for the count pass: lane q accumulates cutoff q's count.
+// (Sinks also take at(first candidate of the step, the cell's image shift)
+// before each step; only the batched record sink uses it.)
 struct CountSink {
   const CutoffSet* cs;
   uint32_t cnt;  // lane q: count of cutoff q
+  __device__ __forceinline__ void at(int32_t, const int32_t*) {}
   __device__ __forceinline__ void operator()(bool hit, double d2, int32_t, int32_t, const int32_t*) {
     const int lane = threadIdx.x & 31;
     const int k = cs->k;
@@ -54,6 +57,7 @@ struct EmitSinkT {
   const Targets* t;
   int64_t cursor;  // lane q: next slot of cutoff q
   int64_t idx_off = 0;  // added to both atom indices
+  __device__ __forceinline__ void at(int32_t, const int32_t*) {}
   __device__ __forceinline__ void operator()(bool hit, double d2, int32_t io, int32_t jo,
                                              const int32_t* s) {
     const int lane = threadIdx.x & 31;

@@ -561,6 +561,9 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos) {
       if (mask_have > mask_cap) mask_cap = mask_have;
       b.task_hdr = slot<int4>(c, kSlotTaskHdr, max_tasks);
       b.masks = slot<uint32_t>(c, kSlotMasks, mask_cap);
+      const bool chunk_boxes = (double)n / (double)nb >= kChunkPruneMinPerBin;
+      b.cbox = chunk_boxes ? slot<float4>(c, kSlotCbox, 2 * (size_t)n) : nullptr;
+      if (chunk_boxes && !b.cbox) return fail(NLB_ERR_NOMEM, "device allocation failed");
       b.mask_cap = mask_cap;
       b.mask_top = zeroed ? reinterpret_cast<unsigned long long*>(zeroed + 2 * nb + 2) : nullptr;
       if (!b.p32 || !b.sbin || !b.groups || !b.irr_list || !b.irr || !b.counters ||

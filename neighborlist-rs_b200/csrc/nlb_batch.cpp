@@ -241,11 +241,25 @@ struct FastBatchArgs {
   int64_t* d_bounds;  // nullptr: no per-system offsets
   BatchItems bw;
   int64_t cap;
+  bool use_rec;          // single cutoff: count pass records hits, expansion writes the list
+  BatchRecords rec;
+  int32_t* rec_flags;    // rec.seg_top / overflow / need_recompute (zeroed per batch)
 };
 
 void issue_emit_fast(Ctx& c, const FastBatchArgs& a, const std::vector<double>& rc_sq,
-                     cudaStream_t s) {
+                     cudaStream_t s, bool recompute = false) {
   const int32_t k = (int32_t)rc_sq.size();
+  if (a.use_rec && !recompute) {
+    EmitTargets t;
+    std::memset(&t, 0, sizeof(t));
+    t.src[0] = static_cast<int64_t*>(c.batch_out[0].p);
+    t.dst[0] = static_cast<int64_t*>(c.batch_out[1].p);
+    t.sh[0] = static_cast<int32_t*>(c.batch_out[2].p);
+    t.capacity = a.cap;
+    t.scan_error = a.scan_tmp + 1;
+    launch_batch_expand(a.rec, a.plans, a.d_pos, a.offs, a.row, t, s);
+    return;
+  }
   for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
     const CutoffSet cs = make_pass(rc_sq, g0, a.disjoint);
     EmitTargets t;
@@ -268,20 +282,27 @@ void issue_batch_fast(Ctx& c, const FastBatchArgs& a, const std::vector<double>&
   const int32_t k = (int32_t)rc_sq.size();
   cudaMemsetAsync(a.flags, 0, sizeof(int32_t) * 3, s);
   cudaMemsetAsync(a.counts, 0, sizeof(uint32_t) * (size_t)k * a.row, s);
+  if (a.use_rec) cudaMemsetAsync(a.rec_flags, 0, sizeof(int32_t) * 3, s);
+  c.mark(0);
   launch_plan(a.d_pos, a.d_starts, 0, a.n_sys, a.d_cells, a.d_pbcs, a.d_has, a.rc_max,
               g_bf_threshold.load(), a.multi ? 1 : 0, 0, a.plans, a.flags, s);
+  c.mark(1);
   for (int32_t g0 = 0; g0 < k; g0 += kMaxCutoffsPerPass) {
     const CutoffSet cs = make_pass(rc_sq, g0, a.disjoint);
     cudaMemsetAsync(a.flags + 1, 0, sizeof(int32_t) * 2, s);
     launch_batch_count(a.plans, a.bw, a.d_pos, cs, a.counts + (size_t)g0 * a.row, a.row,
-                       a.flags + 1, s);
+                       a.flags + 1, s, a.use_rec ? &a.rec : nullptr);
   }
+  c.mark(2);
   exclusive_scan_u32(a.counts, (int64_t)k * a.row, a.offs, a.scan_tmp, s);
   if (a.d_bounds)
     for (int32_t q = 0; q < k; ++q)
       launch_sys_bounds(a.plans, a.n_sys, a.offs + (size_t)q * a.row, a.row,
                         a.d_bounds + (size_t)q * (a.n_sys + 1), s);
+  c.mark(3);
+  c.mark(4);
   issue_emit_fast(c, a, rc_sq, s);
+  c.mark(5);
 }
 
 // Grows the k arenas (src, dst, shift per list) to `cap` edges each.
@@ -315,7 +336,6 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
                       const std::vector<int32_t>& order, bool disjoint, bool multi,
                       nlb_result* outs, int64_t* sys_offsets, bool* handled) {
   *handled = false;
-  if (c.prof) return Status{NLB_OK};
   cudaStream_t s = c.stream;
   const int32_t ns = (int32_t)starts.size() - 1;
   const int32_t k = (int32_t)rc_sq.size();
@@ -358,6 +378,26 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
   if (have > cap) cap = have;
   if (!arenas_for(c, k, cap, s)) return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
   a.cap = cap;
+  // Hit records (single cutoff): at most one segment per atom plus one per
+  // 32 records, and a record holds at least one of the <= cap edges.
+  a.use_rec = k == 1;
+  if (a.use_rec) {
+    const int64_t segs = run_atoms + cap / 32 + 1024;
+    if (segs > INT32_MAX / 2) {
+      a.use_rec = false;
+    } else {
+      a.rec.seg_cap = (int)segs;
+      a.rec.seg_hdr = slot<int4>(c, kSlotBatch0 + 13, (size_t)segs);
+      a.rec.rec = slot<uint32_t>(c, kSlotBatch0 + 14, (size_t)segs * 96);
+      a.rec.meta = slot<SlotMeta>(c, kSlotBatch0 + 15, (size_t)run_atoms);
+      a.rec_flags = slot<int32_t>(c, kSlotBatch0 + 12, 3);
+      if (!a.rec.seg_hdr || !a.rec.rec || !a.rec.meta || !a.rec_flags)
+        return fail(NLB_ERR_NOMEM, "device allocation failed");
+      a.rec.seg_top = a.rec_flags;
+      a.rec.overflow = a.rec_flags + 1;
+      a.rec.need_recompute = a.rec_flags + 2;
+    }
+  }
 
   // Everything the issued work depends on.
   std::vector<unsigned char> key;
@@ -371,7 +411,8 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
     put(key, c.batch_out[3 * q + 1].p);
     put(key, c.batch_out[3 * q + 2].p);
   }
-  const bool same = !scan_stall_armed() && key == bg.key;
+  // (Phase profiling times directly launched kernels: no graph then.)
+  const bool same = !scan_stall_armed() && !c.prof && key == bg.key;
   bool launched = false;
   if (same && bg.exec) {
     if (cudaGraphLaunch(bg.exec, s) == cudaSuccess) {
@@ -415,13 +456,17 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
 
   // One synchronisation: list totals, plan errors, the scan's error word,
   // per-system offsets.
-  if (k + 3 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
+  if (k + 4 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
   cudaError_t e = cudaMemcpy2DAsync(c.h_small, sizeof(int64_t), a.offs, sizeof(int64_t) * a.row,
                                     sizeof(int64_t), (size_t)k + 1, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(c.h_small + k + 1, a.flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(c.h_small + k + 2, a.scan_tmp + 1, sizeof(int64_t),
+                        cudaMemcpyDeviceToHost, s);
+  c.h_small[k + 3] = 0;
+  if (e == cudaSuccess && a.use_rec)  // the expansion found incomplete records
+    e = cudaMemcpyAsync(c.h_small + k + 3, a.rec.need_recompute, sizeof(int32_t),
                         cudaMemcpyDeviceToHost, s);
   std::vector<int64_t> bounds;
   if (e == cudaSuccess && sys_offsets) {
@@ -431,6 +476,11 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "batched build");
+  if (c.prof) {
+    c.prof_pending_count = true;
+    c.prof_pending_emit = true;
+    c.harvest();
+  }
   if (c.h_small[k + 2] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
   const int32_t plan_err = (int32_t)(c.h_small[k + 1] & 0xffffffff);
   if (plan_err == 1) return fail(NLB_ERR_VALUE, "Cell matrix is not invertible");
@@ -442,12 +492,17 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
     m_max = std::max(m_max, m[q]);
   }
   if (m_max > cap) {
-    // An arena was too small (nothing was written): grow and emit again.
+    // An arena was too small (nothing was written): grow and emit again
+    // (recomputing: the records were sized for the smaller arena).
     a.cap = m_max + m_max / 8 + 1024;
     if (!arenas_for(c, k, a.cap, s))
       return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
-    issue_emit_fast(c, a, rc_sq, s);
+    issue_emit_fast(c, a, rc_sq, s, true);
     bg.key.clear();  // arena pointers changed
+  } else if ((c.h_small[k + 3] & 0xffffffff) != 0) {
+    // The records were incomplete (a segment or an image shift did not fit):
+    // the expansion wrote nothing; recompute the list.
+    issue_emit_fast(c, a, rc_sq, s, true);
   }
   bg.last_m = m_max;
 

@@ -110,6 +110,8 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   const int64_t max_tasks = (n / 32 + std::min<int64_t>(n, nb) + 1) * cells;
   b.task_hdr = slot<int4>(c, kSlotTaskHdr, max_tasks);
   b.masks = slot<uint32_t>(c, kSlotMasks, mask_cap);
+  const bool chunk_boxes = nb > 0 && (double)n / (double)nb >= kChunkPruneMinPerBin;
+  b.cbox = chunk_boxes ? slot<float4>(c, kSlotCbox, 2 * (size_t)n) : nullptr;
   b.mask_cap = mask_cap;
   b.bin_start = slot<int64_t>(c, kSlotBinStart, nb + 1);
   b.key = slot<uint64_t>(c, kSlotKey, n);
@@ -135,7 +137,7 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   if (!b.rank_of_bin || !zeroed || !b.bin_start || !b.key || !b.rank || !b.skey || !b.sidx ||
       !b.skey2 || !b.sidx2 || !b.px || !b.py || !b.pz || !b.meta || !b.p32 || !b.sbin ||
       !b.groups || !b.irr_list || !b.irr || !b.scan_tmp || !sp.counts || !sp.offs ||
-      !sp.out_src || !sp.out_sh || !b.task_hdr || !b.masks)
+      !sp.out_src || !sp.out_sh || !b.task_hdr || !b.masks || (chunk_boxes && !b.cbox))
     return fail(NLB_ERR_NOMEM, "device allocation failed");
   return Status{NLB_OK};
 }

@@ -52,6 +52,7 @@ enum Slot : int {
   kSlotCounters,
   kSlotTaskHdr,
   kSlotMasks,
+  kSlotCbox,
   kSlotBatch0,  // first slot owned by the batched path
   kSlotCount = kSlotBatch0 + 32,
 };

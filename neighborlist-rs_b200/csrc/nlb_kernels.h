@@ -80,7 +80,18 @@ struct GridBuffers {
   uint32_t* masks;
   unsigned long long* mask_top;
   int64_t mask_cap;
+  // Optional (nullptr: no chunk pruning), set on grids dense enough that a
+  // bin holds several 32-atom chunks: FP32 bounding box, in its bin's frame,
+  // of the chunk of up to 32 sorted atoms starting at slot j (every chunk
+  // starts at its bin's first slot + a multiple of 32): cbox[2j] = lower
+  // corner, cbox[2j + 1] = upper corner.  Written by the build; the count
+  // pass skips a (group, chunk) pair whose boxes are farther apart than the
+  // guard band's upper bound by more than the band's width.
+  float4* cbox;
 };
+
+// Grids with at least this many atoms per bin on average get chunk boxes.
+constexpr double kChunkPruneMinPerBin = 64.0;
 
 constexpr int64_t kFusedBinScanMax = 65536;
 
@@ -237,10 +248,29 @@ struct BatchItems {
 // Host: builds the item list (upload it and set w.items before launching).
 void plan_batch_items(const int64_t* sizes, int n_sys, const BatchShape& shape,
                       std::vector<int2>& items, BatchItems& w);
-// counts[q * row + slot + p]; work2[0..1] must be zero on entry.
+// Hit records of a single-cutoff batched count pass, expanded into the list
+// by launch_batch_expand instead of a recomputing emit pass.  seg_top,
+// overflow and need_recompute must be zero on entry; capacity: seg_cap
+// segments of 32 records (3 words each), meta: one per run slot.
+struct BatchRecords {
+  int4* seg_hdr;         // {run slot of the atom, its edges in earlier segments, records, system}
+  uint32_t* rec;         // [seg_cap * 32 * 3]
+  SlotMeta* meta;        // sorted meta per run slot (orig: index within the system)
+  int* seg_top;          // segments used
+  int* overflow;         // 1: records incomplete (the emit pass must recompute)
+  int* need_recompute;   // set by the expansion when it found the overflow flag
+  int seg_cap;
+};
+
+// counts[q * row + slot + p]; work2[0..1] must be zero on entry.  With rec
+// (single-cutoff passes only) the pass also writes hit records.
 void launch_batch_count(const SysPlan* plans, const BatchItems& w, const double* pos,
                         const CutoffSet& cs, uint32_t* counts, int64_t row, int* work2,
-                        cudaStream_t s);
+                        cudaStream_t s, const BatchRecords* rec = nullptr);
+// Writes the single-cutoff list from the records (t: src/dst/sh[0], base[0],
+// index options, capacity and scan_error as for launch_batch_emit).
+void launch_batch_expand(const BatchRecords& rb, const SysPlan* plans, const double* pos,
+                         const int64_t* offs, int64_t row, const EmitTargets& t, cudaStream_t s);
 void launch_batch_emit(const SysPlan* plans, const BatchItems& w, const double* pos,
                        const CutoffSet& cs, const int64_t* offs, int64_t row,
                        const EmitTargets& t, int* work2, cudaStream_t s);

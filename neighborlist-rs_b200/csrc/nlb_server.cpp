@@ -359,6 +359,8 @@ class Server {
     s[11] = us_emit_wait.load();
     s[12] = us_large.load();
     s[13] = cancelled_;
+    s[14] = us_queue_wait_;
+    s[15] = max_queued_;
   }
 
  private:
@@ -435,7 +437,12 @@ class Server {
         if (stop_) break;
         items = take_work();
         if (items.empty()) continue;
-        for (Req* r : items) r->status = 1;
+        const double t_start = now_s();
+        for (Req* r : items) {
+          r->status = 1;
+          us_queue_wait_ += (int64_t)(1e6 * (t_start - r->t_submit));
+        }
+        max_queued_ = std::max<int64_t>(max_queued_, (int64_t)queue_.size() + (int64_t)items.size());
         ++batches_;
         max_batch_seen_ = std::max<int64_t>(max_batch_seen_, (int64_t)items.size());
       }
@@ -594,7 +601,7 @@ class Server {
     const size_t bytes_tab =
         ((sizeof(int64_t) + 9 * sizeof(double) + 3 + 1 + sizeof(double)) * (size_t)(ns + 1) + 63) &
         ~(size_t)63;
-    const size_t bytes_back = sizeof(int64_t) * (size_t)(ns + 3);
+    const size_t bytes_back = sizeof(int64_t) * (size_t)(ns + 4);
     if (staging_bytes_ < bytes_pos + bytes_tab + bytes_back) {
       pinned_release(staging_);
       staging_bytes_ = (bytes_pos + bytes_tab + bytes_back) * 2;
@@ -653,6 +660,29 @@ class Server {
     int64_t* bounds = slot<int64_t>(*c, kSlotBatch0 + 11, ns + 1);
     if (!plans || !flags || !counts || !offs || !scan_tmp || !bounds)
       return fail(NLB_ERR_NOMEM, "device allocation failed");
+    // Hit records for the expansion pass (a kind whose launch shape is
+    // decided: one count pass), sized by the admission estimates; a batch
+    // whose records do not fit recomputes in its emit pass instead.
+    BatchRecords rb;
+    std::memset(&rb, 0, sizeof(rb));
+    const bool use_rec = !trials.timed;
+    int32_t* rec_flags = nullptr;
+    if (use_rec) {
+      size_t est_edges = 0;
+      for (Req* r : items) est_edges += r->est_result / 28;
+      const int64_t segs = total_atoms + (int64_t)(est_edges / 32) + 1024;
+      rb.seg_cap = (int)std::min<int64_t>(segs, INT32_MAX / 2);
+      rb.seg_hdr = slot<int4>(*c, kSlotBatch0 + 13, (size_t)rb.seg_cap);
+      rb.rec = slot<uint32_t>(*c, kSlotBatch0 + 14, (size_t)rb.seg_cap * 96);
+      rb.meta = slot<SlotMeta>(*c, kSlotBatch0 + 15, (size_t)std::max<int64_t>(total_atoms, 1));
+      rec_flags = slot<int32_t>(*c, kSlotBatch0 + 12, 3);
+      if (!rb.seg_hdr || !rb.rec || !rb.meta || !rec_flags)
+        return fail(NLB_ERR_NOMEM, "device allocation failed");
+      rb.seg_top = rec_flags;
+      rb.overflow = rec_flags + 1;
+      rb.need_recompute = rec_flags + 2;
+      cudaMemsetAsync(rec_flags, 0, sizeof(int32_t) * 3, s);
+    }
     cudaMemsetAsync(flags, 0, sizeof(int32_t) * 3, s);
     cudaMemsetAsync(counts, 0, sizeof(uint32_t) * row, s);
     launch_plan(d_pos, d_starts, 0, ns, d_cells, d_pbc, d_has, 0.0, g_bf_threshold.load(), 0, 0,
@@ -664,7 +694,8 @@ class Server {
     for (size_t t = 0; t < trials.w.size(); ++t) {
       trials.mark(*c, t);
       if (t > 0) cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
-      launch_batch_count(plans, trials.w[t], d_pos, cs, counts, row, flags + 1, s);
+      launch_batch_count(plans, trials.w[t], d_pos, cs, counts, row, flags + 1, s,
+                         use_rec ? &rb : nullptr);
     }
     trials.mark(*c, trials.w.size());
     exclusive_scan_u32(counts, row, offs, scan_tmp, s);
@@ -674,10 +705,13 @@ class Server {
     int64_t* hb = reinterpret_cast<int64_t*>(staging_ + bytes_pos + bytes_tab);
     int64_t* diag = hb + ns + 1;
     diag[0] = 0;
+    diag[2] = 0;
     cudaError_t e = cudaMemcpyAsync(hb, bounds, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&diag[0], flags, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(&diag[1], scan_tmp + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && use_rec)  // records complete?
+      e = cudaMemcpyAsync(&diag[2], rb.overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     us_stage += us_since(t_mark);
     t_mark = now_s();
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -716,8 +750,12 @@ class Server {
     t.sh[0] = shf;
     t.local_indices = 1;
     t.system_blocks = 1;  // request i: [src | dst] at src + 2 hb[i]
-    cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
-    launch_batch_emit(plans, trials.pick(*c), d_pos, cs, offs, row, t, flags + 1, s);
+    if (use_rec && (diag[2] & 0xffffffff) == 0) {
+      launch_batch_expand(rb, plans, d_pos, offs, row, t, s);
+    } else {
+      cudaMemsetAsync(flags + 1, 0, sizeof(int32_t) * 2, s);
+      launch_batch_emit(plans, trials.pick(*c), d_pos, cs, offs, row, t, flags + 1, s);
+    }
     // Host results of the batch come back in two copies into shared pinned
     // blocks, each request holding slices of them.
     bool any_host = false;
@@ -798,6 +836,8 @@ class Server {
   bool stop_ = false;
   bool paused_ = false;
   int64_t cancelled_ = 0;
+  int64_t us_queue_wait_ = 0;  // sum over started requests of submit -> start (admission wait)
+  int64_t max_queued_ = 0;     // deepest queue seen when work was taken
   int64_t next_id_ = 1;
   int64_t submitted_ = 0, completed_ = 0, failed_ = 0, batches_ = 0, max_batch_seen_ = 0;
   std::vector<std::thread> threads_;

@@ -38,7 +38,7 @@ _lib.nlb_server_destroy.argtypes = [ctypes.c_void_p]
 _NLB_NOT_READY = 4
 _STATS = ("submitted", "completed", "failed", "batches", "reserved_bytes", "queued",
           "largest_batch", "budget_bytes", "us_stage", "us_count_wait", "us_deliver",
-          "us_emit_wait", "us_large", "cancelled")
+          "us_emit_wait", "us_large", "cancelled", "us_queue_wait", "max_queued")
 
 
 class DeviceResult:
