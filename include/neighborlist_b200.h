@@ -168,6 +168,14 @@ int64_t nlb_kernel_launches(void);
  * decided launch shape, buffers, stream) replay their captured graphs. */
 int64_t nlb_graph_replays(void);
 
+/* Single-system, single-cutoff pipeline choice (no counterpart in the
+ * reference).  mode 0 (the default): sparse grids (at most 64 atoms per bin
+ * on average, at most 125 stencil cells) count, place and write their edges
+ * in one launch, denser ones in three (count, offsets scan, emit); mode 1:
+ * always the three-launch pipeline.  Both give identical results.  mode < 0
+ * only queries.  Returns the previous mode, or -1 for an unknown mode. */
+int32_t nlb_single_pipeline(int32_t mode);
+
 /* Failure-detection hook (no counterpart in the reference, which has no
  * device waits).  The device prefix scans wait on their predecessor tiles
  * with bounded polls; when a wait runs out, the scan records an error word,

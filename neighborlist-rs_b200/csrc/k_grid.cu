@@ -68,30 +68,50 @@ __global__ void k_rank_table(GridParams g, int32_t* __restrict__ rank_of_bin) {
 constexpr int kPrepThreads = 256;
 
 // Exclusive scan of the bin histogram by one CTA (kPrepThreads threads):
-// bin_start[b] = sum of counts below b, bin_start[nb] = total.
+// bin_start[b] = sum of counts below b, bin_start[nb] = total.  With
+// group_start, also the exclusive scan of the 32-atom groups per bin
+// (ceil(count / 32)): the canonical index of each bin's first group.
 __device__ void cta_bin_scan(const int32_t* __restrict__ bin_count, int64_t nb,
-                             int64_t* __restrict__ bin_start) {
+                             int64_t* __restrict__ bin_start, int32_t* __restrict__ group_start) {
   __shared__ int64_t warp_tot[kPrepThreads / 32];
+  __shared__ int64_t warp_grp[kPrepThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t per = (nb + kPrepThreads - 1) / kPrepThreads;
   const int64_t b0 = tid * per < nb ? tid * per : nb;
   const int64_t b1 = b0 + per < nb ? b0 + per : nb;
-  int64_t sum = 0;
-  for (int64_t b = b0; b < b1; ++b) sum += __ldcg(&bin_count[b]);
-  int64_t x = sum;  // inclusive scan over the CTA
+  int64_t sum = 0, gsum = 0;
+  for (int64_t b = b0; b < b1; ++b) {
+    const int64_t v = __ldcg(&bin_count[b]);
+    sum += v;
+    gsum += (v + 31) / 32;
+  }
+  int64_t x = sum, gx = gsum;  // inclusive scans over the CTA
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
+    const int64_t gy = __shfl_up_sync(0xffffffffu, gx, o);
+    if (lane >= o) {
+      x += y;
+      gx += gy;
+    }
   }
-  if (lane == 31) warp_tot[warp] = x;
+  if (lane == 31) {
+    warp_tot[warp] = x;
+    warp_grp[warp] = gx;
+  }
   __syncthreads();
-  int64_t before = 0;
-  for (int w = 0; w < warp; ++w) before += warp_tot[w];
-  int64_t run = before + x - sum;
+  int64_t before = 0, gbefore = 0;
+  for (int w = 0; w < warp; ++w) {
+    before += warp_tot[w];
+    gbefore += warp_grp[w];
+  }
+  int64_t run = before + x - sum, grun = gbefore + gx - gsum;
   for (int64_t b = b0; b < b1; ++b) {
+    const int64_t v = __ldcg(&bin_count[b]);
     bin_start[b] = run;
-    run += __ldcg(&bin_count[b]);
+    run += v;
+    if (group_start) group_start[b] = (int32_t)grun;
+    grun += (v + 31) / 32;
   }
   if (tid == kPrepThreads - 1) bin_start[nb] = before + x;
 }
@@ -102,7 +122,8 @@ __global__ void __launch_bounds__(kPrepThreads)
     k_prep(GridParams g, const double* __restrict__ pos, int64_t n,
            const int32_t* __restrict__ rank_of_bin, uint64_t* __restrict__ key,
            int32_t* __restrict__ rank, int32_t* __restrict__ bin_count,
-           int64_t* __restrict__ bin_start, int32_t* __restrict__ done) {
+           int64_t* __restrict__ bin_start, int32_t* __restrict__ done,
+           int32_t* __restrict__ group_start) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
     const AtomWrap w = wrap_atom(g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
@@ -120,7 +141,7 @@ __global__ void __launch_bounds__(kPrepThreads)
   __syncthreads();
   if (!last) return;
   __threadfence();
-  cta_bin_scan(bin_count, g.total_bins, bin_start);
+  cta_bin_scan(bin_count, g.total_bins, bin_start, group_start);
 }
 
 __global__ void k_scatter(const uint64_t* __restrict__ key, const int32_t* __restrict__ rank,
@@ -179,7 +200,7 @@ __global__ void __launch_bounds__(kSortThreads)
               SlotMeta* __restrict__ meta, float4* __restrict__ p32, int32_t* __restrict__ sbin,
               GroupRec* __restrict__ groups, int32_t* __restrict__ irr_list,
               uint8_t* __restrict__ irr, int32_t* __restrict__ counters,
-              float4* __restrict__ cbox) {
+              float4* __restrict__ cbox, const int32_t* __restrict__ group_start) {
   __shared__ uint64_t sk[kSortCap];
   __shared__ int32_t sv[kSortCap];
   pdl_wait();
@@ -312,7 +333,10 @@ __global__ void __launch_bounds__(kSortThreads)
   }
   if (p32 && threadIdx.x == 0) {
     const int ng = (int)((cnt + 31) / 32);
-    const int base = atomicAdd(&counters[0], ng);
+    // (canonical position when the group starts are known: bins in rank
+    // order, 32-atom runs in slot order)
+    const int placed = atomicAdd(&counters[0], ng);
+    const int base = group_start ? group_start[r] : placed;
     const int32_t lin = sbin[s];
     GroupRec gr;
     gr.end = (int32_t)e;
@@ -385,13 +409,14 @@ void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const 
   const bool fused = b.build_done != nullptr && g.total_bins <= kFusedBinScanMax;
   k_prep<<<(unsigned)((n + kPrepThreads - 1) / kPrepThreads), kPrepThreads, 0, s>>>(
       g, pos, n, b.rank_of_bin, b.key, b.rank, b.bin_count, b.bin_start,
-      fused ? b.build_done : nullptr);
+      fused ? b.build_done : nullptr, fused ? b.group_start : nullptr);
   if (!fused) exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
   launch_pdl(k_scatter, dim3((unsigned)((n + T - 1) / T)), dim3(T), 0, s, b.key, b.rank, n,
              b.bin_start, b.bin_fill, b.skey, b.sidx);
   launch_pdl(k_binsort, dim3((unsigned)g.total_bins), dim3(kSortThreads), 0, s, g, pos,
              b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta, b.p32,
-             b.sbin, b.groups, b.irr_list, b.irr, b.counters, b.cbox);
+             b.sbin, b.groups, b.irr_list, b.irr, b.counters, b.cbox,
+             fused ? b.group_start : nullptr);
   note_launches(3);
 }
 

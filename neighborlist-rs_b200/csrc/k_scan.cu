@@ -195,6 +195,14 @@ void scan_impl(const TIn* in, int64_t n, int64_t* out, int64_t* tmp, cudaStream_
 
 bool scan_stall_armed() { return tl_withhold_tile >= 0; }
 
+bool take_scan_stall(int32_t* tile, int32_t* spin_limit) {
+  if (tl_withhold_tile < 0) return false;
+  *tile = tl_withhold_tile;
+  *spin_limit = tl_withhold_spins;
+  tl_withhold_tile = -1;
+  return true;
+}
+
 void arm_scan_stall(int32_t tile, int32_t spin_limit) {
   tl_withhold_tile = tile;
   tl_withhold_spins = spin_limit;

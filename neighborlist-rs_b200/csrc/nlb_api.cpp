@@ -802,8 +802,14 @@ Status download_results(Ctx& c, const std::vector<int64_t>& m, const DevLists& L
     Status st = alloc_result(m[q], &r);
     if (!st.ok()) return st;
     if (m[q] == 0) continue;
-    cudaError_t e = cudaMemcpyAsync(r.edge_index, L.src[q], sizeof(int64_t) * 2 * m[q],
+    // [src | dst] in one copy when the destinations follow the sources.
+    const bool joined = L.dst[q] == L.src[q] + m[q];
+    cudaError_t e = cudaMemcpyAsync(r.edge_index, L.src[q],
+                                    sizeof(int64_t) * (joined ? 2 : 1) * m[q],
                                     cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess && !joined)
+      e = cudaMemcpyAsync(r.edge_index + m[q], L.dst[q], sizeof(int64_t) * m[q],
+                          cudaMemcpyDeviceToHost, c.stream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(r.shift, L.sh[q], sizeof(int32_t) * 3 * m[q], cudaMemcpyDeviceToHost,
                           c.stream);
@@ -855,11 +861,11 @@ Status run_single(const double* pos, int64_t n, const double* cell9, const uint8
   if (!st.ok()) return st;
   if (fast_eligible(sp)) {
     int64_t m = 0;
-    st = run_fast(*c, sp, d_pos, &m);
+    st = run_fast(*c, sp, d_pos, &m, false);  // (host copies: no [src | dst] layout needed)
     if (!st.ok()) return st;
     DevLists L;
     L.src.assign(1, sp.out_src);
-    L.dst.assign(1, sp.out_src + m);
+    L.dst.assign(1, sp.out_dst);
     L.sh.assign(1, sp.out_sh);
     st = download_results(*c, std::vector<int64_t>(1, m), L, sp.order, outs);
     if (!st.ok()) nlb_result_free(&outs[0]);
@@ -1274,6 +1280,12 @@ void nlb_set_stream(void* stream) { tl_user_stream = static_cast<cudaStream_t>(s
 int64_t nlb_kernel_launches(void) { return g_launches.load(); }
 
 int64_t nlb_graph_replays(void) { return g_graph_replays.load(); }
+
+int32_t nlb_single_pipeline(int32_t mode) {
+  if (mode < 0) return single_pipeline_mode();
+  if (mode > 1) return -1;
+  return set_single_pipeline_mode(mode);
+}
 
 int nlb_debug_scan_stall(int32_t tile, int32_t spin_limit) {
   if (tile < 0 || spin_limit < 1)

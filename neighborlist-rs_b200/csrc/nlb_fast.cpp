@@ -9,6 +9,14 @@
 // end, and only if the arena was too small does it grow it and run the emit
 // pass again (the counts and offsets are still in place).
 //
+// On sparse grids (at most 64 atoms per bin on average, at most 125 stencil
+// cells) the count, offsets scan and emit are one launch instead
+// (k_fused.cu): the build stores the groups in canonical order, one CTA per
+// group counts, finds its output offset by a look-back over the groups
+// before it and writes its block; the edge total again comes from device
+// memory, and an arena that was too small makes the host grow it and run the
+// fused launch again.
+//
 // The first call with a given set of launch parameters runs the work
 // directly; a repeated call with identical parameters (same positions
 // buffer, cell, cutoff, sizes and workspace) captures the sequence into a
@@ -16,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -37,6 +46,8 @@ struct FastKey {
   int64_t mask_cap;
   int32_t need_rank;
   int32_t prof;
+  int32_t fused;
+  int32_t contiguous;
 };
 
 struct FastState {
@@ -69,7 +80,12 @@ int64_t estimate_edges(const SystemPlan& sp, double rc) {
   return (int64_t)std::min(est, 4.0e12);
 }
 
+std::atomic<int32_t> g_pipeline_mode{0};
+
 }  // namespace
+
+int32_t single_pipeline_mode() { return g_pipeline_mode.load(); }
+int32_t set_single_pipeline_mode(int32_t mode) { return g_pipeline_mode.exchange(mode); }
 
 void release_fast_states() {
   for (FastState& fs : tl_states) {
@@ -98,9 +114,17 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   // 2 nb + 6), so a single
   // memset at the start clears everything and the kernels follow each other
   // directly.
-  sp.zeroed_words = 2 * (size_t)nb + 6 + 2 * (size_t)scan_tmp_elems(row);
+  // (Fused launch: its ticket, error and look-back words and its total take
+  // the scan state's place.)
+  const int64_t max_groups = n / 32 + std::min<int64_t>(n, nb) + 1;
+  sp.fused_words = 2 + max_groups + 1;
+  sp.zeroed_words = 2 * (size_t)nb + 6 +
+                    2 * (size_t)(sp.fused ? sp.fused_words : scan_tmp_elems(row));
   int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, sp.zeroed_words);
   sp.scan_state = zeroed ? reinterpret_cast<int64_t*>(zeroed + 2 * nb + 6) : nullptr;
+  sp.fused_state = reinterpret_cast<uint64_t*>(sp.scan_state);
+  sp.fused_total = sp.fused && zeroed ? sp.scan_state + 2 + max_groups : nullptr;
+  b.group_start = sp.fused ? slot<int32_t>(c, kSlotGroupStart, nb) : nullptr;
   b.bin_count = zeroed;
   b.bin_fill = zeroed ? zeroed + nb : nullptr;
   b.counters = zeroed ? zeroed + 2 * nb : nullptr;
@@ -108,11 +132,12 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   b.build_done = zeroed ? zeroed + 2 * nb + 4 : nullptr;
   b.emit_queue = zeroed ? reinterpret_cast<uint32_t*>(zeroed + 2 * nb + 5) : nullptr;
   const int64_t max_tasks = (n / 32 + std::min<int64_t>(n, nb) + 1) * cells;
-  b.task_hdr = slot<int4>(c, kSlotTaskHdr, max_tasks);
-  b.masks = slot<uint32_t>(c, kSlotMasks, mask_cap);
+  // (The fused launch needs no task headers, masks, counts or offsets.)
+  b.task_hdr = slot<int4>(c, kSlotTaskHdr, sp.fused ? 1 : max_tasks);
+  b.masks = slot<uint32_t>(c, kSlotMasks, sp.fused ? 1 : mask_cap);
   const bool chunk_boxes = nb > 0 && (double)n / (double)nb >= kChunkPruneMinPerBin;
   b.cbox = chunk_boxes ? slot<float4>(c, kSlotCbox, 2 * (size_t)n) : nullptr;
-  b.mask_cap = mask_cap;
+  b.mask_cap = sp.fused ? 0 : mask_cap;
   b.bin_start = slot<int64_t>(c, kSlotBinStart, nb + 1);
   b.key = slot<uint64_t>(c, kSlotKey, n);
   b.rank = slot<int32_t>(c, kSlotRank, n);
@@ -130,16 +155,45 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   b.irr_list = slot<int32_t>(c, kSlotIrrList, n);
   b.irr = slot<uint8_t>(c, kSlotIrr, n);
   b.scan_tmp = slot<int64_t>(c, kSlotScanTmp, scan_tmp_elems(std::max<int64_t>(row, nb)));
-  sp.counts = slot<uint32_t>(c, kSlotCounts, row);
-  sp.offs = slot<int64_t>(c, kSlotOffs, row + 1);
+  sp.counts = slot<uint32_t>(c, kSlotCounts, sp.fused ? 1 : row);
+  sp.offs = slot<int64_t>(c, kSlotOffs, sp.fused ? 1 : row + 1);
   sp.out_src = slot<int64_t>(c, kSlotOutEi, 2 * (size_t)capacity);
   sp.out_sh = slot<int32_t>(c, kSlotOutSh, 3 * (size_t)capacity);
+  int64_t* dst_arena = sp.fused ? slot<int64_t>(c, kSlotOutDst, (size_t)capacity) : nullptr;
+  if (sp.fused && (!dst_arena || !b.group_start))
+    return fail(NLB_ERR_NOMEM, "device allocation failed");
   if (!b.rank_of_bin || !zeroed || !b.bin_start || !b.key || !b.rank || !b.skey || !b.sidx ||
       !b.skey2 || !b.sidx2 || !b.px || !b.py || !b.pz || !b.meta || !b.p32 || !b.sbin ||
       !b.groups || !b.irr_list || !b.irr || !b.scan_tmp || !sp.counts || !sp.offs ||
       !sp.out_src || !sp.out_sh || !b.task_hdr || !b.masks || (chunk_boxes && !b.cbox))
     return fail(NLB_ERR_NOMEM, "device allocation failed");
   return Status{NLB_OK};
+}
+
+FusedOut fused_targets(Ctx& c, const SystemPlan& sp, int64_t capacity) {
+  FusedOut o;
+  std::memset(&o, 0, sizeof(o));
+  o.src = sp.out_src;
+  o.dst = static_cast<int64_t*>(c.bufs[kSlotOutDst].p);
+  o.sh = sp.out_sh;
+  o.capacity = capacity;
+  o.state = sp.fused_state;
+  o.total = sp.fused_total;
+  o.spin_limit = kFusedSpinLimit;
+  o.withhold = -1;
+  int32_t tile = 0, spins = 0;
+  if (take_scan_stall(&tile, &spins)) {  // failure-detection hook
+    o.withhold = tile;
+    o.spin_limit = spins;
+  }
+  return o;
+}
+
+// The fused launch (and the move of the destinations behind the sources).
+void issue_fused(Ctx& c, SystemPlan& sp, int64_t capacity, bool contiguous) {
+  const FusedOut o = fused_targets(c, sp, capacity);
+  launch_pair_fused(sp.grid, sp.gb, (int32_t)stencil_cells_of(sp.grid), sp.band, o, c.stream);
+  if (contiguous) launch_move_dst(o.src, o.dst, o.total, capacity, c.stream);
 }
 
 EmitTargets fast_targets(const SystemPlan& sp, int64_t capacity) {
@@ -154,14 +208,24 @@ EmitTargets fast_targets(const SystemPlan& sp, int64_t capacity) {
 }
 
 // Issues the whole pipeline on c.stream (no host synchronisation).
-void issue_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t capacity) {
+void issue_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t capacity,
+                bool contiguous) {
   cudaStream_t s = c.stream;
   const int64_t n = sp.n;
-  const int64_t nb = sp.grid.total_bins;
   c.mark(0);
   cudaMemsetAsync(sp.gb.bin_count, 0, sizeof(int32_t) * sp.zeroed_words, s);
   launch_grid_build(sp.grid, d_pos, n, sp.gb, s, !sp.rank_cached);
   c.mark(1);
+  if (sp.fused) {
+    // (Phases: counting and offsets are part of the one launch, timed with
+    // the emit.)
+    c.mark(2);
+    c.mark(3);
+    c.mark(4);
+    issue_fused(c, sp, capacity, contiguous);
+    c.mark(5);
+    return;
+  }
   launch_pair_count(sp.grid, sp.gb, n, sp.band, sp.counts, s);
   c.mark(2);
   exclusive_scan_u32_zeroed(sp.counts, sp.row, sp.offs, sp.scan_state, s);
@@ -173,8 +237,12 @@ void issue_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t capacity) {
 
 // Runs the fast pipeline for a planned single-cutoff cell-list system and
 // leaves M edges in sp.out_src ([src | dst]) / sp.out_sh.
-Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
+Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, bool contiguous) {
   FastState& fs = state_for(c);
+  const int64_t n_cells = stencil_cells_of(sp.grid);
+  sp.fused = single_pipeline_mode() == 0 && n_cells <= kFusedMaxCells &&
+             sp.grid.total_bins > 0 && sp.grid.total_bins <= kFusedBinScanMax &&
+             (double)sp.n / (double)sp.grid.total_bins <= kFusedMaxPerBin;
   const double rc = std::sqrt(sp.rc_sq[0]);
   int64_t capacity = std::max<int64_t>(
       {4096, (int64_t)(1.25 * (double)fs.last_m), (int64_t)(1.5 * (double)estimate_edges(sp, rc))});
@@ -201,6 +269,8 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
   key.mask_cap = mask_cap;
   key.need_rank = sp.rank_cached ? 0 : 1;
   key.prof = c.prof ? 1 : 0;
+  key.fused = sp.fused ? 1 : 0;
+  key.contiguous = contiguous ? 1 : 0;
 
   // (An armed failure-detection hook must reach a directly launched scan,
   // never a captured or replayed one.)
@@ -226,7 +296,7 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
     cudaGraph_t graph = nullptr;
     const int64_t l0 = nlb_kernel_launches();
     if (cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      issue_fast(c, sp, d_pos, capacity);
+      issue_fast(c, sp, d_pos, capacity, contiguous);
       if (cudaStreamEndCapture(c.stream, &graph) == cudaSuccess && graph) {
         if (cudaGraphInstantiate(&fs.exec, graph, 0) != cudaSuccess) fs.exec = nullptr;
         cudaGraphDestroy(graph);
@@ -245,19 +315,20 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
       cudaGraphExecDestroy(fs.exec);
       fs.exec = nullptr;
     }
-    issue_fast(c, sp, d_pos, capacity);
+    issue_fast(c, sp, d_pos, capacity, contiguous);
   }
   fs.key = key;
   fs.have_key = true;
   for (int a = 0; a < 3; ++a) c.rank_nb[a] = sp.grid.nb[a];
 
   // One synchronisation: total edges and the scan's wait-error word.
-  cudaError_t e = cudaMemcpyAsync(c.h_small, sp.offs + sp.row, sizeof(int64_t),
-                                  cudaMemcpyDeviceToHost, c.stream);
-  if (e == cudaSuccess)
+  cudaError_t e = cudaMemcpyAsync(c.h_small, sp.fused ? sp.fused_total : sp.offs + sp.row,
+                                  sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess)  // the scan's (or the fused look-back's) wait-error word
     e = cudaMemcpyAsync(c.h_small + 1, sp.scan_state + 1, sizeof(int64_t),
                         cudaMemcpyDeviceToHost, c.stream);
-  if (e == cudaSuccess)
+  c.h_small[2] = 0;
+  if (e == cudaSuccess && !sp.fused)
     e = cudaMemcpyAsync(c.h_small + 2, sp.gb.mask_top, sizeof(int64_t), cudaMemcpyDeviceToHost,
                         c.stream);
   // Grids too large for k_prep's own bin scan use a separate scan (state in
@@ -282,11 +353,27 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out) {
     sp.out_src = slot<int64_t>(c, kSlotOutEi, 2 * (size_t)cap2);
     sp.out_sh = slot<int32_t>(c, kSlotOutSh, 3 * (size_t)cap2);
     if (!sp.out_src || !sp.out_sh) return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
-    launch_pair_emit(sp.grid, sp.gb, sp.n, sp.band, sp.offs, fast_targets(sp, cap2), c.stream);
-    e = cudaStreamSynchronize(c.stream);
-    if (e != cudaSuccess) return cuda_fail(e, "emit pass");
+    if (sp.fused) {
+      // The fused launch counts again: clear its ticket, look-back words and
+      // total first.
+      if (!slot<int64_t>(c, kSlotOutDst, (size_t)cap2))
+        return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
+      cudaMemsetAsync(sp.fused_state, 0, sizeof(uint64_t) * (size_t)sp.fused_words, c.stream);
+      issue_fused(c, sp, cap2, contiguous);
+      e = cudaMemcpyAsync(c.h_small + 1, sp.scan_state + 1, sizeof(int64_t),
+                          cudaMemcpyDeviceToHost, c.stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "fused pass");
+      if (c.h_small[1] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+    } else {
+      launch_pair_emit(sp.grid, sp.gb, sp.n, sp.band, sp.offs, fast_targets(sp, cap2), c.stream);
+      e = cudaStreamSynchronize(c.stream);
+      if (e != cudaSuccess) return cuda_fail(e, "emit pass");
+    }
     fs.have_key = false;  // workspace pointers changed
   }
+  sp.out_dst = sp.fused && !contiguous ? static_cast<int64_t*>(c.bufs[kSlotOutDst].p)
+                                       : sp.out_src + m;
   fs.last_m = m;
   fs.last_mask_words = c.h_small[2];
   *m_out = m;

@@ -53,6 +53,8 @@ enum Slot : int {
   kSlotTaskHdr,
   kSlotMasks,
   kSlotCbox,
+  kSlotGroupStart,
+  kSlotOutDst,
   kSlotBatch0,  // first slot owned by the batched path
   kSlotCount = kSlotBatch0 + 32,
 };
@@ -162,6 +164,11 @@ struct SystemPlan {
   size_t zeroed_words = 0;        // fast path: int32 words cleared at the start of a run
   int64_t* out_src = nullptr;   // fast path: [src | dst] arena
   int32_t* out_sh = nullptr;    // fast path: shift arena
+  int64_t* out_dst = nullptr;   // fast path: where the M destinations are after run_fast
+  bool fused = false;           // fast path: one-launch count + offsets + emit (k_fused.cu)
+  uint64_t* fused_state = nullptr;  // its ticket / error / look-back words (in the zeroed block)
+  int64_t* fused_total = nullptr;   // its edge total (in the zeroed block)
+  int64_t fused_words = 0;          // 64-bit words of fused_state + total
   CutoffSet pass(int32_t g0) const;
 };
 
@@ -183,8 +190,15 @@ Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& 
 // Single-cutoff cell-list pipeline with one synchronisation, replayed as a
 // CUDA graph for repeated identical calls (nlb_fast.cpp).  Requires
 // sp.method == kCellList and sp.fp32; leaves the M edges in sp.out_src
-// ([src | dst]) and sp.out_sh.
-Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out);
+// (sources), sp.out_dst (destinations) and sp.out_sh.  contiguous = true
+// puts the destinations right behind the sources (sp.out_dst = out_src + M,
+// the [src | dst] layout); otherwise they may stay in a separate array.
+Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out,
+                bool contiguous = true);
+// Single-system pipeline choice: 0 = automatic (the one-launch kernel on
+// sparse grids), 1 = always the three-launch pair-task pipeline.
+int32_t single_pipeline_mode();
+int32_t set_single_pipeline_mode(int32_t mode);  // returns the previous mode
 inline bool fast_eligible(const SystemPlan& sp) {
   return sp.method == Method::kCellList && sp.fp32 && sp.rc_sq.size() == 1;
 }

@@ -19,6 +19,9 @@ int64_t scan_tmp_elems(int64_t n);
 // (then record the error word and finish).  One-shot.
 void arm_scan_stall(int32_t tile, int32_t spin_limit);
 bool scan_stall_armed();
+// Takes the armed hook for a launch that is not a scan (the fused search's
+// look-back over groups); false when none is armed.
+bool take_scan_stall(int32_t* tile, int32_t* spin_limit);
 void exclusive_scan_u32(const uint32_t* in, int64_t n, int64_t* out, int64_t* tmp,
                         cudaStream_t s);
 void exclusive_scan_i32(const int32_t* in, int64_t n, int64_t* out, int64_t* tmp,
@@ -88,6 +91,10 @@ struct GridBuffers {
   // pass skips a (group, chunk) pair whose boxes are farther apart than the
   // guard band's upper bound by more than the band's width.
   float4* cbox;
+  // Optional ([total_bins], written by k_prep's own bin scan): canonical
+  // index of each bin's first group; the build then stores groups[] in
+  // canonical order (bins in rank order, runs in slot order).
+  int32_t* group_start;
 };
 
 // Grids with at least this many atoms per bin on average get chunk boxes.
@@ -159,6 +166,36 @@ struct PairBands {
 };
 // Stencils above this many cells use the per-atom FP64 kernels.
 constexpr int64_t kPairMaxCells = 1024;
+// ---- k_fused.cu : count + offsets + emit of the single-cutoff list in one
+// launch (one CTA per 32-atom group, decoupled look-back over the groups).
+// Needs the groups in canonical order (GridBuffers::group_start set for the
+// build) and at most kFusedMaxCells stencil cells.
+constexpr int32_t kFusedMaxCells = 125;
+// Grids with more atoms per bin than this keep the three-launch pipeline
+// (their hit masks would not fit in shared memory).
+constexpr double kFusedMaxPerBin = 64.0;
+struct FusedOut {
+  int64_t* src;       // [capacity] sources
+  int64_t* dst;       // [capacity] destinations (a separate array)
+  int32_t* sh;        // [3 capacity] shifts
+  int64_t capacity;   // a group whose block does not fit writes nothing
+  uint64_t* state;    // zeroed: [0] group ticket, [1] error word, [2 + g] group g's look-back word
+  int64_t* total;     // receives M
+  int32_t spin_limit; // polls of one look-back wait before it gives up
+  int32_t withhold;   // failure-detection hook: this group never publishes (-1: none)
+};
+__host__ __device__ inline size_t fused_cells_bytes(int32_t n_cells) {
+  return ((size_t)88 * (size_t)n_cells + 15) & ~(size_t)15;
+}
+size_t fused_smem_bytes(int32_t n_cells);
+// Moves the M destinations of the fused kernel behind the M sources (reads
+// M from *total; nothing when M > capacity).
+void launch_move_dst(int64_t* src, const int64_t* dst, const int64_t* total, int64_t capacity,
+                     cudaStream_t s);
+constexpr int32_t kFusedSpinLimit = 1 << 22;
+void launch_pair_fused(const GridParams& g, const GridBuffers& b, int32_t n_cells,
+                       const GuardBand& band, const FusedOut& o, cudaStream_t s);
+
 // Returns false when the FP32 test cannot be made safe for this grid (the
 // band would be too wide); callers then use the FP64 kernels.
 bool make_guard_band(const GridParams& g, double rc, GuardBand& band);

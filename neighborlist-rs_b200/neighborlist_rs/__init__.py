@@ -482,6 +482,20 @@ def pinned_stats() -> dict:
     return dict(zip(_PINNED_STATS, (int(x) for x in buf)))
 
 
+_lib.nlb_single_pipeline.argtypes = [ctypes.c_int32]
+_lib.nlb_single_pipeline.restype = ctypes.c_int32
+
+
+def set_single_pipeline(mode: int | None) -> int:
+    """Single-system pipeline: 0 (or None) = automatic (one launch for count,
+    offsets and emit on sparse grids), 1 = always the three-launch pair-task
+    pipeline.  Identical results either way; returns the previous mode."""
+    r = int(_lib.nlb_single_pipeline(0 if mode is None else int(mode)))
+    if r < 0:
+        raise ValueError(f"no single-system pipeline mode {mode}")
+    return r
+
+
 def set_batch_shape(shape: int | None) -> int:
     """Pin launch shape `shape` of the batched kernels (None: tune per kind of
     batch, the default).  Returns the number of shapes."""
