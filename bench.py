@@ -487,24 +487,37 @@ def run_b200(args):
     # per-phase CUDA-event times -> roofline of the dominant kernel
     ph = dt.phases(max(5, args.steps // 3))
     peak, peak_kind = peaks()
-    # Algorithmic bytes per launch: emit writes the 28 B/edge output and reads
-    # the sorted SoA + per-(atom, cell) offsets once; count reads the sorted
-    # FP32 coordinates and writes one count per (atom, stencil cell).
+    # Algorithmic bytes per launch: the emit (or the one-launch kernel) writes
+    # the 28 B/edge output and reads the sorted SoA (positions, FP32
+    # coordinates, meta) once; the count pass of the three-launch pipeline
+    # reads the sorted FP32 coordinates and writes one count per (atom,
+    # stencil cell).
     cells = 27  # stencil cells of this grid (n_search = 1 on every axis)
     bytes_emit = 28 * m_step + 48 * n
     bytes_count = 16 * n + 4 * cells * n
-    # The emit pass has the largest share of the ncu launch list; the count
-    # pass, within a few us of it in live timing and issue-bound, is reported
-    # beside it.
+    fused = ph["count"] < 1e-4 and ph["scan"] < 1e-4  # one-launch pipeline (sparse grids)
     dominant = "emit"
     alg = bytes_emit
     achieved = alg / (ph[dominant] * 1e-3) / 1e9
     # DRAM bytes (read + write) per launch of the same kernel on the same
     # workload, from an ncu capture (not measured by this run).
-    traffic, capture = ncu_traffic(args.rc, dominant)
+    traffic, capture = ncu_traffic(args.rc, "fused" if fused else dominant)
     count_traffic, _ = ncu_traffic(args.rc, "count")
-    kernel_name = {"emit": "k_pair_tasks<1> (emit pass)",
-                   "count": "k_pair_tasks<0> (count pass)"}[dominant]
+    if fused:
+        kernel_name = ("k_pair_fused (count, offsets by look-back over groups, emit: one launch) "
+                       "+ k_move_dst (destinations behind the sources)")
+        second = {"note": "no separate count pass or offsets scan: both are inside k_pair_fused"}
+    else:
+        # The emit pass has the largest share of the ncu launch list; the
+        # count pass, within a few us of it in live timing and issue-bound,
+        # is reported beside it.
+        kernel_name = "k_pair_tasks<1> (emit pass)"
+        second = {"kernel": "k_pair_tasks<0> (count pass)",
+                  "bound": "instruction issue (61-78 % issue-active in ncu)",
+                  "algorithmic_bytes": bytes_count, "kernel_ms": ph["count"],
+                  "achieved_gbs": bytes_count / (ph["count"] * 1e-3) / 1e9,
+                  "traffic": count_traffic}
+    step_bytes = 24 * n + 72 + 28 * m_step
 
     # e2e through the reference-facing call (host buffers)
     nl.set_stream(None)
@@ -530,12 +543,12 @@ def run_b200(args):
                      "algorithmic_bytes": alg, "kernel_ms": ph[dominant], "traffic": traffic,
                      "traffic_source": f"ncu capture {capture} (committed traffic table)"
                      if traffic is not None else None,
-                     "phases_ms": ph,
-                     "count_pass": {"kernel": "k_pair_tasks<0> (count pass)",
-                                    "bound": "instruction issue (61-78 % issue-active in ncu)",
-                                    "algorithmic_bytes": bytes_count, "kernel_ms": ph["count"],
-                                    "achieved_gbs": bytes_count / (ph["count"] * 1e-3) / 1e9,
-                                    "traffic": count_traffic}},
+                     "phases_ms": ph, "pipeline": "one launch" if fused else "three launches",
+                     "count_pass": second,
+                     "whole_step": {"algorithmic_bytes": step_bytes,
+                                    "ms": ms_max / args.steps,
+                                    "achieved_gbs": step_bytes / (ms_max / args.steps * 1e-3) / 1e9,
+                                    "frac": step_bytes / (ms_max / args.steps * 1e-3) / 1e9 / peak}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * n + 72,
                 "d2h_bytes_per_step": 28 * m_e2e},
     }
