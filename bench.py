@@ -130,7 +130,48 @@ def _case_multi(nl, torch, steps, warmup):
             "ms_per_call": 1e3 * (time.perf_counter() - t0) / steps}
 
 
+def _case_every_kernel(nl, torch, steps, warmup):
+    """Each kernel of the library on a modest workload, `steps` rounds after
+    `warmup` rounds (for an ncu capture of every kernel): the headline build
+    in both single-system pipelines, rc 14 (chunk boxes), an isolated
+    device-resident build (auto-box bounds), a 512-system batch (plan, count
+    with records, expansion), the output options (directed list, vectors,
+    distances) and Verlet updates."""
+    W = workloads()
+    from neighborlist_rs.verlet import VerletList
+
+    pos, rows = headline_system()
+    cell = nl.PyCell(rows.T.tolist())
+    d = torch.from_numpy(pos).cuda()
+    iso = torch.from_numpy(W.isolated_cube()).cuda()
+    pb, bb, cb = W.concat_batch(W.uneven_batch(n_systems=512, seed=71))
+    vl = VerletList(6.0, 1.0)
+    moved = d + 0.01
+
+    def one_round():
+        nl.build_neighborlists_torch(cell, d, 6.0)
+        nl.set_single_pipeline(1)
+        nl.build_neighborlists_torch(cell, d, 6.0)
+        nl.set_single_pipeline(0)
+        nl.build_neighborlists_torch(cell, d, 14.0)
+        nl.build_neighborlists_torch(None, iso, 6.0)
+        nl.build_neighborlists_batch(pb, bb, cells=cb, cutoff=5.0)
+        nl.build_neighborlists_torch(cell, d, 6.0, directed=True, vectors=True, distances=True)
+        vl.update(cell, d)
+        vl.update(cell, moved)
+        torch.cuda.synchronize()
+
+    for _ in range(warmup):
+        one_round()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one_round()
+    vl.close()
+    return {"rounds": steps, "ms_per_round": 1e3 * (time.perf_counter() - t0) / max(steps, 1)}
+
+
 CASES = {
+    "every_kernel": _case_every_kernel,
     "cluster_liquid_rc6": _case_device(6.0),
     "cluster_liquid_rc14": _case_device(14.0),
     "uneven_batch_4096": _case_batch,
