@@ -377,7 +377,9 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
   const int64_t have = arena_capacity(c, k);
   if (have > cap) cap = have;
   if (!arenas_for(c, k, cap, s)) return fail(NLB_ERR_NOMEM, "device allocation for the edge lists failed");
-  a.cap = cap;
+  // The arenas' actual capacity (so that repeated calls see the same value
+  // once the arenas stop growing).
+  a.cap = arena_capacity(c, k);
   // Hit records (single cutoff): at most one segment per atom plus one per
   // 32 records, and a record holds at least one of the <= cap edges.
   a.use_rec = k == 1;

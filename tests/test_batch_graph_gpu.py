@@ -41,21 +41,28 @@ def test_repeated_batch_replays_a_graph(nl, oracle):
     ocells = [None if not c.any() else (c.T, PBC3) for c in cells]
     (ref,) = oracle.search_batch(pos, batch, ocells, [5.0], nthreads=16)
     r0 = replays(nl)
-    for k in range(5):  # tuning call(s), a direct call, a capture, replays
-        got = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=5.0,
-                                           return_offsets=k % 2 == 1)
+    for k in range(5):  # tuning call, direct calls while the arenas settle, capture, replay
+        got = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=5.0)
         assert_same(got, ref, f"call {k}")
     assert replays(nl) - r0 >= 2
+    # With the per-system offset table (a different launch sequence).
+    got = nl.build_neighborlists_batch(pos, batch, cells=cells, cutoff=5.0, return_offsets=True)
+    assert_same(got, ref, "offsets call")
+    counts = np.bincount(batch[ref[0][0]], minlength=1024)
+    assert np.array_equal(got["system_offsets"], np.concatenate([[0], np.cumsum(counts)]))
     # New positions (and cells) of the same shapes reuse the graph.
     rng = np.random.default_rng(52)
     moved = pos + rng.normal(0.0, 0.05, pos.shape)
     cells2 = cells * 1.01
     ocells2 = [None if not c.any() else (c.T, PBC3) for c in cells2]
     (ref2,) = oracle.search_batch(moved, batch, ocells2, [5.0], nthreads=16)
+    for k in range(3):
+        assert_same(nl.build_neighborlists_batch(moved, batch, cells=cells2, cutoff=5.0), ref2,
+                    f"moved call {k}")
     r1 = replays(nl)
     for k in range(2):
         assert_same(nl.build_neighborlists_batch(moved, batch, cells=cells2, cutoff=5.0), ref2,
-                    f"moved call {k}")
+                    f"moved replay {k}")
     assert replays(nl) - r1 == 2
 
 
