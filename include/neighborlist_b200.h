@@ -194,6 +194,10 @@ int nlb_debug_scan_stall(int32_t tile, int32_t spin_limit);
  * pass, and returns the number of profiled calls. */
 void nlb_profile(int enable);
 int64_t nlb_profile_read(double* ms);
+/* Host wall time of profiled batched builds of small systems (ms, summed):
+ * input upload, device work from issue to its synchronisation, result
+ * copies, the whole call; returns the number of profiled calls. */
+int64_t nlb_profile_host(double* ms);
 
 /* Launch shapes of the batched kernels (no counterpart in the reference,
  * whose batch path has no launch configuration).  Batches are tuned per kind

@@ -1371,9 +1371,18 @@ void nlb_profile(int enable) {
   Ctx* c = nullptr;
   if (get_ctx(&c).ok()) {
     c->prof_ms[0] = c->prof_ms[1] = c->prof_ms[2] = c->prof_ms[3] = 0.0;
+    for (double& v : c->prof_host_ms) v = 0.0;
     c->prof_calls = 0;
     c->prof_pending_count = c->prof_pending_emit = false;
   }
+}
+
+int64_t nlb_profile_host(double* ms) {
+  Ctx* c = nullptr;
+  if (!get_ctx(&c).ok()) return -1;
+  if (ms)
+    for (int i = 0; i < 4; ++i) ms[i] = c->prof_host_ms[i];
+  return c->prof_calls;
 }
 
 int64_t nlb_profile_read(double* ms) {

@@ -10,6 +10,7 @@
 // margin and mic_safe from the largest cutoff).
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -21,6 +22,14 @@
 namespace nlb {
 
 extern std::atomic<uint64_t> g_bf_threshold;
+
+namespace {
+double wall_ms() {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+}  // namespace
 
 namespace {
 
@@ -456,6 +465,7 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
   }
   bg.key.swap(key);
 
+  const double t_issue = wall_ms();
   // One synchronisation: list totals, plan errors, the scan's error word,
   // per-system offsets.
   if (k + 4 > kSmallHost) return fail(NLB_ERR_VALUE, "too many cutoffs");
@@ -478,10 +488,12 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "batched build");
+  const double t_synced = wall_ms();
   if (c.prof) {
     c.prof_pending_count = true;
     c.prof_pending_emit = true;
     c.harvest();
+    c.prof_host_ms[1] += t_synced - t_issue;
   }
   if (c.h_small[k + 2] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
   const int32_t plan_err = (int32_t)(c.h_small[k + 1] & 0xffffffff);
@@ -532,6 +544,7 @@ Status run_small_fast(Ctx& c, const double* d_pos, const std::vector<int64_t>& s
     for (int32_t q = 0; q < k; ++q) nlb_result_free(&outs[order[q]]);
     return cuda_fail(e, "batched emit");
   }
+  if (c.prof) c.prof_host_ms[2] += wall_ms() - t_synced;
   return Status{NLB_OK};
 }
 
@@ -581,6 +594,7 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
   Ctx* c = nullptr;
   Status st = get_ctx(&c);
   if (!st.ok()) return st;
+  const double t_call = wall_ms();
   cudaStream_t s = c->stream;
   double* d_pos = nullptr;
   st = upload_positions(*c, pos, n, &d_pos);
@@ -612,9 +626,14 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
   for (int32_t i = 0; i < n_sys && all_small; ++i)
     all_small = starts[i + 1] - starts[i] <= kBatchMaxAtoms;
   if (all_small) {
+    const double t_up = wall_ms();
     bool handled = false;
     st = run_small_fast(*c, d_pos, starts, d_starts, d_cells, d_pbcs, d_has, rc_max, rc_sq, order,
                         disjoint, multi, outs, sys_offsets, &handled);
+    if (c->prof && handled) {
+      c->prof_host_ms[0] += t_up - t_call;
+      c->prof_host_ms[3] += wall_ms() - t_call;
+    }
     if (!st.ok() || handled) return st;
   }
 

@@ -92,6 +92,9 @@ struct Ctx {
   bool prof_pending_emit = false;
   cudaEvent_t ev[6] = {};
   double prof_ms[4] = {0, 0, 0, 0};
+  // Host wall time of batched builds while profiling (ms, accumulated):
+  // input upload, issue-to-sync of the device work, result copies, whole call.
+  double prof_host_ms[4] = {0, 0, 0, 0};
   // Bins per axis of the rank table currently in kSlotRankTab (-1: none).
   int32_t rank_nb[3] = {-1, -1, -1};
   // Hit-mask words the last multi-cutoff pair-task count pass needed.

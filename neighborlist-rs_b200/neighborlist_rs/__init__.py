@@ -283,31 +283,28 @@ def build_multi_from_ase(atoms, cutoffs, labels=None, disjoint=False):
     return build_neighborlists_multi(cell, positions, cutoffs, labels, disjoint)
 
 
-def _batch_cells(cells, batch):
-    """Monotonic check, system count and the (B,3,3) cells -> C arrays
-    (src/python_api.rs:353-407): a zero matrix means isolated (auto-box); any
-    other cell is transposed from ASE rows and gets pbc (T, T, T)."""
-    n_sys = 1
-    cur = int(batch[0])
-    # vectorised form of the reference's scan
-    d = np.diff(batch.astype(np.int64))
-    if (d < 0).any():
+def _batch_cells(cells, batch, need_count=False):
+    """Monotonic check and the (B,3,3) cells -> C arrays (src/python_api.rs:
+    353-407): a zero matrix means isolated (auto-box); any other cell is
+    transposed from ASE rows and gets pbc (T, T, T).  Every given cell is
+    passed on; the library splits the systems and reports "Expected at least
+    {n} cells, but got {m}" when there are fewer cells than systems.  The
+    system count is computed here only when the caller needs it."""
+    b1, b0 = batch[1:], batch[:-1]
+    if (b1 < b0).any():
         raise ValueError("Batch IDs must be monotonic (non-decreasing)")
-    n_sys = 1 + int((d != 0).sum())
-    del cur
+    n_sys = 1 + int(np.count_nonzero(b1 != b0)) if need_count else -1
     if cells is None:
         return n_sys, None, None, None, 0
     if not isinstance(cells, np.ndarray) or cells.ndim != 3 or cells.dtype != np.float64:
         raise TypeError("cells must be a 3-D numpy array of float64")
-    if cells.shape[0] < n_sys:
-        raise ValueError(f"Expected at least {n_sys} cells, but got {cells.shape[0]}")
-    c = np.asarray(cells[:n_sys])
-    if c.shape[1:] != (3, 3):
+    if cells.shape[1:] != (3, 3):
         raise ValueError("cells must have shape (B, 3, 3)")
-    has = np.any(c != 0.0, axis=(1, 2)).astype(np.uint8)
-    h9 = np.ascontiguousarray(np.transpose(c, (0, 2, 1)).reshape(n_sys, 9))
-    pbcs = np.ones((n_sys, 3), np.uint8)
-    return n_sys, h9, pbcs, has, n_sys
+    nc = cells.shape[0]
+    has = np.any(cells != 0.0, axis=(1, 2)).astype(np.uint8)
+    h9 = np.ascontiguousarray(np.transpose(cells, (0, 2, 1)).reshape(nc, 9))
+    pbcs = np.ones((nc, 3), np.uint8)
+    return n_sys, h9, pbcs, has, nc
 
 
 def build_neighborlists_batch(positions, batch, cells=None, cutoff=5.0, parallel=True, *,
@@ -328,7 +325,7 @@ def build_neighborlists_batch(positions, batch, cells=None, cutoff=5.0, parallel
         if return_offsets:
             res["system_offsets"] = np.zeros(1, np.int64)
         return res
-    n_sys, h9, pbcs, has, nc = _batch_cells(cells, b)
+    n_sys, h9, pbcs, has, nc = _batch_cells(cells, b, need_count=return_offsets)
     r = _Result()
     cells_args = (h9.ctypes.data_as(_dp) if h9 is not None else None,
                   pbcs.ctypes.data_as(_u8p) if pbcs is not None else None,
@@ -365,7 +362,7 @@ def build_neighborlists_batch_multi(positions, batch, cells=None, cutoffs=(5.0,)
         labels = [str(x) for x in labels]
         if len(labels) != len(cs):
             raise ValueError("Length of labels must match length of cutoffs")
-    n_sys, h9, pbcs, has, nc = _batch_cells(cells, b)
+    n_sys, h9, pbcs, has, nc = _batch_cells(cells, b, need_count=return_offsets)
     k = len(cs)
     carr = np.ascontiguousarray(np.array(cs, dtype=np.float64))
     outs = (_Result * k)()
@@ -459,6 +456,8 @@ _lib.nlb_kernel_launches.restype = ctypes.c_int64
 _lib.nlb_profile.argtypes = [ctypes.c_int]
 _lib.nlb_profile_read.argtypes = [_dp]
 _lib.nlb_profile_read.restype = ctypes.c_int64
+_lib.nlb_profile_host.argtypes = [_dp]
+_lib.nlb_profile_host.restype = ctypes.c_int64
 _lib.nlb_batch_shape.argtypes = [ctypes.c_int32]
 _lib.nlb_batch_shape.restype = ctypes.c_int32
 _lib.nlb_batch_shape_info.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
@@ -541,6 +540,13 @@ def kernel_launches() -> int:
 
 def profile(enable: bool) -> None:
     _lib.nlb_profile(int(bool(enable)))
+
+
+def profile_host_read():
+    """(calls, {upload, device, results, total} host ms of profiled batched builds)."""
+    ms = np.zeros(4, np.float64)
+    calls = int(_lib.nlb_profile_host(ms.ctypes.data_as(_dp)))
+    return calls, dict(zip(("upload", "device", "results", "total"), ms.tolist()))
 
 
 def profile_read():
