@@ -536,7 +536,7 @@ def run_b200(args):
     cells = 27  # stencil cells of this grid (n_search = 1 on every axis)
     bytes_emit = 28 * m_step + 48 * n
     bytes_count = 16 * n + 4 * cells * n
-    fused = ph["count"] < 1e-4 and ph["scan"] < 1e-4  # one-launch pipeline (sparse grids)
+    fused = nl.last_single_pipeline() == 0  # one-launch pipeline (sparse grids)
     dominant = "emit"
     alg = bytes_emit
     achieved = alg / (ph[dominant] * 1e-3) / 1e9

@@ -175,6 +175,9 @@ int64_t nlb_graph_replays(void);
  * always the three-launch pipeline.  Both give identical results.  mode < 0
  * only queries.  Returns the previous mode, or -1 for an unknown mode. */
 int32_t nlb_single_pipeline(int32_t mode);
+/* The pipeline the calling thread's last single-cutoff cell-list build took:
+ * 0 = one launch, 1 = three launches, -1 = none yet. */
+int32_t nlb_last_single_pipeline(void);
 
 /* Failure-detection hook (no counterpart in the reference, which has no
  * device waits).  The device prefix scans wait on their predecessor tiles

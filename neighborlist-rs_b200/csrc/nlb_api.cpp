@@ -1352,6 +1352,8 @@ int64_t nlb_kernel_launches(void) { return g_launches.load(); }
 
 int64_t nlb_graph_replays(void) { return g_graph_replays.load(); }
 
+int32_t nlb_last_single_pipeline(void) { return last_single_pipeline(); }
+
 int32_t nlb_single_pipeline(int32_t mode) {
   if (mode < 0) return single_pipeline_mode();
   if (mode > 1) return -1;

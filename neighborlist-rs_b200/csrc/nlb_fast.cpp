@@ -84,7 +84,12 @@ std::atomic<int32_t> g_pipeline_mode{0};
 
 }  // namespace
 
+namespace {
+thread_local int32_t tl_last_fused = -1;  // pipeline of this thread's last fast-path build
+}  // namespace
+
 int32_t single_pipeline_mode() { return g_pipeline_mode.load(); }
+int32_t last_single_pipeline() { return tl_last_fused; }
 int32_t set_single_pipeline_mode(int32_t mode) { return g_pipeline_mode.exchange(mode); }
 
 void release_fast_states() {
@@ -243,6 +248,7 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, boo
   sp.fused = single_pipeline_mode() == 0 && n_cells <= kFusedMaxCells &&
              sp.grid.total_bins > 0 && sp.grid.total_bins <= kFusedBinScanMax &&
              (double)sp.n / (double)sp.grid.total_bins <= kFusedMaxPerBin;
+  tl_last_fused = sp.fused ? 0 : 1;
   const double rc = std::sqrt(sp.rc_sq[0]);
   int64_t capacity = std::max<int64_t>(
       {4096, (int64_t)(1.25 * (double)fs.last_m), (int64_t)(1.5 * (double)estimate_edges(sp, rc))});

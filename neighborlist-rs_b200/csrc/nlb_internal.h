@@ -202,6 +202,9 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out,
 // sparse grids), 1 = always the three-launch pair-task pipeline.
 int32_t single_pipeline_mode();
 int32_t set_single_pipeline_mode(int32_t mode);  // returns the previous mode
+// Pipeline of the calling thread's last single-cutoff cell-list build:
+// 0 = one launch, 1 = three launches, -1 = none yet.
+int32_t last_single_pipeline();
 inline bool fast_eligible(const SystemPlan& sp) {
   return sp.method == Method::kCellList && sp.fp32 && sp.rc_sq.size() == 1;
 }

@@ -483,6 +483,13 @@ def pinned_stats() -> dict:
 
 _lib.nlb_single_pipeline.argtypes = [ctypes.c_int32]
 _lib.nlb_single_pipeline.restype = ctypes.c_int32
+_lib.nlb_last_single_pipeline.restype = ctypes.c_int32
+
+
+def last_single_pipeline() -> int:
+    """Pipeline of this thread's last single-cutoff cell-list build: 0 = one
+    launch, 1 = three launches, -1 = none yet."""
+    return int(_lib.nlb_last_single_pipeline())
 
 
 def set_single_pipeline(mode: int | None) -> int:
