@@ -224,7 +224,10 @@ __device__ void f_irregular(const GridParams& g, const GridBuffers& b, int32_t n
   }
 }
 
-__global__ void __launch_bounds__(kFThreads, 2)
+// Four CTAs per SM (64 registers): every group of a ~10k-atom system is then
+// in flight at once (with three per SM the last ~7 % of the groups waited
+// for a second round).
+__global__ void __launch_bounds__(kFThreads, 4)
     k_pair_fused(GridParams g, GridBuffers b, int32_t n_cells, GuardBand band, FusedOut o) {
   extern __shared__ __align__(16) unsigned char fsm[];
   FCell* cells = reinterpret_cast<FCell*>(fsm);
@@ -236,7 +239,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
   __shared__ int2 st_w[kFWarps][16];
   __shared__ SlotMeta lmeta[32];
   __shared__ int64_t abase[33];
-  __shared__ int32_t s_ticket, s_irr, s_big, s_skip;
+  __shared__ int32_t s_ticket, s_irr, s_big, s_skip, s_cell;
   __shared__ int64_t s_G;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const float lo = band.lo, hi = band.hi;
@@ -266,7 +269,8 @@ __global__ void __launch_bounds__(kFThreads, 2)
       w = dadd(w, dmul(g.basis[1][k], (double)grp.by));
       cb[k] = dadd(w, dmul(g.basis[2][k], (double)grp.bz));
     }
-    for (int c = tid; c < n_cells; c += kFThreads) {
+    // (cell c on lane c / 8 of warp c % 8: the FP64 work spread over the warps)
+    for (int c = (tid & 31) * kFWarps + (tid >> 5); c < n_cells; c += kFThreads) {
       FCell d;
       f_describe(g, b, grp.bx, grp.by, grp.bz, c, d, cb);
       d.mbase = -1;
@@ -287,6 +291,7 @@ __global__ void __launch_bounds__(kFThreads, 2)
         big |= nc >= (1 << kFJBits);
       }
       s_big = big;
+      s_cell = 0;
     }
     __syncthreads();
 
@@ -295,7 +300,12 @@ __global__ void __launch_bounds__(kFThreads, 2)
     const float4 a = b.p32[p];
     const int32_t io = __float_as_int(a.w);
     const double xi = b.px[p], yi = b.py[p], zi = b.pz[p];
-    for (int c = warp; c < n_cells; c += kFWarps) {
+    // (cells handed out one at a time: warps that drew cheap cells take more)
+    for (;;) {
+      int c = 0;
+      if (lane == 0) c = atomicAdd(&s_cell, 1);
+      c = __shfl_sync(0xffffffffu, c, 0);
+      if (c >= n_cells) break;
       const FCell& cell = cells[c];
       const bool live = mine && !(norm2(dsub(cell.cs[0], xi), dsub(cell.cs[1], yi),
                                         dsub(cell.cs[2], zi)) > g.prune_sq);
@@ -392,7 +402,13 @@ __global__ void __launch_bounds__(kFThreads, 2)
     if (!s_skip && E > 0 && !s_irr && !s_big) {
       for (int64_t w0 = 0; w0 < E; w0 += kFStage) {
         const int64_t w1 = E - w0 < kFStage ? E : w0 + kFStage;
-        for (int c = warp; c < n_cells; c += kFWarps) {
+        if (tid == 0) s_cell = 0;
+        __syncthreads();
+        for (;;) {
+          int c = 0;
+          if (lane == 0) c = atomicAdd(&s_cell, 1);
+          c = __shfl_sync(0xffffffffu, c, 0);
+          if (c >= n_cells) break;
           const FCell& cell = cells[c];
           const int64_t start = abase[lane] + pre[c * 32 + lane];
           const int64_t cntc = (int64_t)pre[(c + 1) * 32 + lane] - pre[c * 32 + lane];
