@@ -331,8 +331,9 @@ __global__ void __launch_bounds__(kFThreads, 4)
     }
     __syncthreads();
 
-    // 3. offsets: cells within each atom, atoms within the group, the group
-    //    within the list (decoupled look-back over the groups before it)
+    // 3. offsets: cells within each atom and atoms within the group (warp 0),
+    //    whose total E is published at once for the groups after this one
+    const bool publish = t != o.withhold;  // false only under the test hook
     if (warp == 0) {
       uint32_t run = 0;
       for (int c = 0; c < n_cells; ++c) {
@@ -348,15 +349,61 @@ __global__ void __launch_bounds__(kFThreads, 4)
         if (lane >= s) x += y;
       }
       abase[lane] = x - (int64_t)run;
-      const int64_t E = __shfl_sync(0xffffffffu, x, 31);
-      if (lane == 31) abase[32] = E;
+      const int64_t E0 = __shfl_sync(0xffffffffu, x, 31);
+      if (lane == 31) abase[32] = E0;
+      if (lane == 0 && publish)
+        f_store(&gstate[t], (t == 0 ? kFInclusive : kFAggregate) | ((uint64_t)E0 & kFValueMask));
+    }
+    if (tid == 0) s_cell = 0;
+    __syncthreads();
+    const int64_t E = abase[32];
+    const bool staged = E > 0 && !s_irr && !s_big;
+
+    // Stages the entries [w0, w1) of the group's block in canonical order
+    // (every calling warp takes cells from s_cell).
+    auto build_window = [&](int64_t w0, int64_t w1) {
+      for (;;) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(&s_cell, 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= n_cells) break;
+        const FCell& cell = cells[c];
+        const int64_t start = abase[lane] + pre[c * 32 + lane];
+        const int64_t cntc = (int64_t)pre[(c + 1) * 32 + lane] - pre[c * 32 + lane];
+        const bool need = cntc > 0 && start < w1 && start + cntc > w0;
+        if (!__any_sync(0xffffffffu, need)) continue;
+        const bool shifted = (cell.sh[0] | cell.sh[1] | cell.sh[2]) != 0;
+        const int32_t io_adj = shifted ? io - 1 : io;
+        const float ux = cell.t[0] - a.x, uy = cell.t[1] - a.y, uz = cell.t[2] - a.z;
+        const bool live = mine && !(norm2(dsub(cell.cs[0], xi), dsub(cell.cs[1], yi),
+                                          dsub(cell.cs[2], zi)) > g.prune_sq);
+        int64_t pos = start;
+        for (int32_t jb = cell.b0; jb < cell.b1; jb += 32) {
+          uint32_t hits;
+          if (cell.mbase >= 0)
+            hits = masks[cell.mbase + (jb - cell.b0) + lane];
+          else
+            hits = f_chunk(b, cell, jb, ux, uy, uz, io_adj, live, xi, yi, zi, lo, hi, rc_sq,
+                           st_xy[warp], st_z[warp], st_w[warp]);
+          if (!need) hits = 0;
+          while (hits) {
+            const int jj = __ffs(hits) - 1;
+            hits &= hits - 1;
+            if (pos >= w0 && pos < w1)
+              stage[pos - w0] = ((uint32_t)lane << 27) | ((uint32_t)c << kFJBits) |
+                                (uint32_t)(jb - cell.b0 + jj);
+            ++pos;
+          }
+        }
+      }
+    };
+
+    // 3b. the group within the list: warp 0 walks back over the groups
+    //     before it while the other warps stage the block's first window
+    if (warp == 0) {
       int64_t prefix = 0;
       bool failed_any = false;
-      const bool publish = t != o.withhold;  // false only under the test hook
-      if (t == 0) {
-        if (lane == 0 && publish) f_store(&gstate[0], kFInclusive | ((uint64_t)E & kFValueMask));
-      } else {
-        if (lane == 0 && publish) f_store(&gstate[t], kFAggregate | ((uint64_t)E & kFValueMask));
+      if (t > 0) {
         int32_t tt = t - 1;
         for (;;) {
           const int32_t pred = tt - lane;
@@ -394,51 +441,22 @@ __global__ void __launch_bounds__(kFThreads, 4)
         s_skip = failed_any || prefix + E > o.capacity;
         if (t == n_groups - 1) *o.total = failed_any ? 0 : prefix + E;
       }
+    } else if (staged) {
+      build_window(0, E < kFStage ? E : kFStage);
     }
     __syncthreads();
 
     // 4. write the group's block [G, G + E)
-    const int64_t G = s_G, E = abase[32];
-    if (!s_skip && E > 0 && !s_irr && !s_big) {
+    const int64_t G = s_G;
+    if (!s_skip && staged) {
       for (int64_t w0 = 0; w0 < E; w0 += kFStage) {
         const int64_t w1 = E - w0 < kFStage ? E : w0 + kFStage;
-        if (tid == 0) s_cell = 0;
-        __syncthreads();
-        for (;;) {
-          int c = 0;
-          if (lane == 0) c = atomicAdd(&s_cell, 1);
-          c = __shfl_sync(0xffffffffu, c, 0);
-          if (c >= n_cells) break;
-          const FCell& cell = cells[c];
-          const int64_t start = abase[lane] + pre[c * 32 + lane];
-          const int64_t cntc = (int64_t)pre[(c + 1) * 32 + lane] - pre[c * 32 + lane];
-          const bool need = cntc > 0 && start < w1 && start + cntc > w0;
-          if (!__any_sync(0xffffffffu, need)) continue;
-          const bool shifted = (cell.sh[0] | cell.sh[1] | cell.sh[2]) != 0;
-          const int32_t io_adj = shifted ? io - 1 : io;
-          const float ux = cell.t[0] - a.x, uy = cell.t[1] - a.y, uz = cell.t[2] - a.z;
-          const bool live = mine && !(norm2(dsub(cell.cs[0], xi), dsub(cell.cs[1], yi),
-                                            dsub(cell.cs[2], zi)) > g.prune_sq);
-          int64_t pos = start;
-          for (int32_t jb = cell.b0; jb < cell.b1; jb += 32) {
-            uint32_t hits;
-            if (cell.mbase >= 0)
-              hits = masks[cell.mbase + (jb - cell.b0) + lane];
-            else
-              hits = f_chunk(b, cell, jb, ux, uy, uz, io_adj, live, xi, yi, zi, lo, hi, rc_sq,
-                             st_xy[warp], st_z[warp], st_w[warp]);
-            if (!need) hits = 0;
-            while (hits) {
-              const int jj = __ffs(hits) - 1;
-              hits &= hits - 1;
-              if (pos >= w0 && pos < w1)
-                stage[pos - w0] = ((uint32_t)lane << 27) | ((uint32_t)c << kFJBits) |
-                                  (uint32_t)(jb - cell.b0 + jj);
-              ++pos;
-            }
-          }
+        if (w0 > 0) {
+          if (tid == 0) s_cell = 0;
+          __syncthreads();
+          build_window(w0, w1);
+          __syncthreads();
         }
-        __syncthreads();
         for (int64_t k = w0 + tid; k < w1; k += kFThreads) {
           const uint32_t v = stage[k - w0];
           const int l = (int)(v >> 27);

@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kPrepThreads)
            const int32_t* __restrict__ rank_of_bin, uint64_t* __restrict__ key,
            int32_t* __restrict__ rank, int32_t* __restrict__ bin_count,
            int64_t* __restrict__ bin_start, int32_t* __restrict__ done,
-           int32_t* __restrict__ group_start) {
+           int32_t* __restrict__ group_start, int32_t* __restrict__ fill) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
     const AtomWrap w = wrap_atom(g, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
@@ -131,13 +131,20 @@ __global__ void __launch_bounds__(kPrepThreads)
     const int32_t r = rank_of_bin[lin];
     key[i] = w.key;
     rank[i] = r;
-    atomicAdd(&bin_count[r], 1);
+    // (the histogram's old value is the atom's place in its bin segment,
+    // before the bin sort)
+    const int32_t at = atomicAdd(&bin_count[r], 1);
+    if (fill) fill[i] = at;
   }
   if (!done) return;
   __shared__ int last;
-  __threadfence();  // this CTA's histogram updates before its completion count
+  // One thread releases the CTA's histogram updates (ordered before it by the
+  // barrier) together with its completion count.
   __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(done, 1) == (int)gridDim.x - 1;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(done, 1) == (int)gridDim.x - 1;
+  }
   __syncthreads();
   if (!last) return;
   __threadfence();
@@ -147,12 +154,12 @@ __global__ void __launch_bounds__(kPrepThreads)
 __global__ void k_scatter(const uint64_t* __restrict__ key, const int32_t* __restrict__ rank,
                           int64_t n, const int64_t* __restrict__ bin_start,
                           int32_t* __restrict__ bin_fill, uint64_t* __restrict__ skey,
-                          int32_t* __restrict__ sidx) {
+                          int32_t* __restrict__ sidx, const int32_t* __restrict__ fill) {
   pdl_wait();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int32_t r = rank[i];
-  const int64_t slot = bin_start[r] + atomicAdd(&bin_fill[r], 1);
+  const int64_t slot = bin_start[r] + (fill ? fill[i] : atomicAdd(&bin_fill[r], 1));
   skey[slot] = key[i];
   sidx[slot] = (int32_t)i;
 }
@@ -211,8 +218,41 @@ __global__ void __launch_bounds__(kSortThreads)
   if (cnt == 0) return;
 
   const int32_t* final_idx = sidx;
+  if (cnt <= 32) {
+    // Bins of at most 32 atoms: one warp sorts them in registers (bitonic
+    // network over the lanes), no shared memory or block barriers.
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      uint64_t k = ~0ull;
+      int32_t v = 0x7fffffff;
+      if (lane < cnt) {
+        k = skey[s + lane];
+        v = sidx[s + lane];
+      }
+      for (int size = 2; size <= 32; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+          const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, stride);
+          const int32_t ov = __shfl_xor_sync(0xffffffffu, v, stride);
+          const bool up = (lane & size) == 0;
+          const bool lower = (lane & stride) == 0;
+          // The lower lane of an ascending pair keeps the smaller element.
+          const bool other_less = pair_less(ok, ov, k, v);
+          const bool take = (lower == up) ? other_less : pair_less(k, v, ok, ov);
+          if (take) {
+            k = ok;
+            v = ov;
+          }
+        }
+      }
+      if (lane < cnt) {
+        skey[s + lane] = k;
+        sidx[s + lane] = v;
+      }
+    }
+    __syncthreads();
+  }
   // Sort chunks of kSortCap in shared memory (the whole bin when it fits).
-  for (int64_t c0 = 0; c0 < cnt; c0 += kSortCap) {
+  for (int64_t c0 = 0; cnt > 32 && c0 < cnt; c0 += kSortCap) {
     const int m = (int)(cnt - c0 < kSortCap ? cnt - c0 : kSortCap);
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
       sk[i] = skey[s + c0 + i];
@@ -409,10 +449,10 @@ void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const 
   const bool fused = b.build_done != nullptr && g.total_bins <= kFusedBinScanMax;
   k_prep<<<(unsigned)((n + kPrepThreads - 1) / kPrepThreads), kPrepThreads, 0, s>>>(
       g, pos, n, b.rank_of_bin, b.key, b.rank, b.bin_count, b.bin_start,
-      fused ? b.build_done : nullptr, fused ? b.group_start : nullptr);
+      fused ? b.build_done : nullptr, fused ? b.group_start : nullptr, b.fill);
   if (!fused) exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
   launch_pdl(k_scatter, dim3((unsigned)((n + T - 1) / T)), dim3(T), 0, s, b.key, b.rank, n,
-             b.bin_start, b.bin_fill, b.skey, b.sidx);
+             b.bin_start, b.bin_fill, b.skey, b.sidx, (const int32_t*)b.fill);
   launch_pdl(k_binsort, dim3((unsigned)g.total_bins), dim3(kSortThreads), 0, s, g, pos,
              b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta, b.p32,
              b.sbin, b.groups, b.irr_list, b.irr, b.counters, b.cbox,

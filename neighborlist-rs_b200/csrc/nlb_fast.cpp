@@ -130,6 +130,7 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   sp.fused_state = reinterpret_cast<uint64_t*>(sp.scan_state);
   sp.fused_total = sp.fused && zeroed ? sp.scan_state + 2 + max_groups : nullptr;
   b.group_start = sp.fused ? slot<int32_t>(c, kSlotGroupStart, nb) : nullptr;
+  b.fill = slot<int32_t>(c, kSlotFill, n);
   b.bin_count = zeroed;
   b.bin_fill = zeroed ? zeroed + nb : nullptr;
   b.counters = zeroed ? zeroed + 2 * nb : nullptr;
@@ -170,7 +171,8 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   if (!b.rank_of_bin || !zeroed || !b.bin_start || !b.key || !b.rank || !b.skey || !b.sidx ||
       !b.skey2 || !b.sidx2 || !b.px || !b.py || !b.pz || !b.meta || !b.p32 || !b.sbin ||
       !b.groups || !b.irr_list || !b.irr || !b.scan_tmp || !sp.counts || !sp.offs ||
-      !sp.out_src || !sp.out_sh || !b.task_hdr || !b.masks || (chunk_boxes && !b.cbox))
+      !sp.out_src || !sp.out_sh || !b.task_hdr || !b.masks || (chunk_boxes && !b.cbox) ||
+      !b.fill)
     return fail(NLB_ERR_NOMEM, "device allocation failed");
   return Status{NLB_OK};
 }

@@ -55,6 +55,7 @@ enum Slot : int {
   kSlotCbox,
   kSlotGroupStart,
   kSlotOutDst,
+  kSlotFill,
   kSlotBatch0,  // first slot owned by the batched path
   kSlotCount = kSlotBatch0 + 32,
 };

@@ -95,6 +95,10 @@ struct GridBuffers {
   // index of each bin's first group; the build then stores groups[] in
   // canonical order (bins in rank order, runs in slot order).
   int32_t* group_start;
+  // Optional ([n]): each atom's place in its bin segment, taken by k_prep
+  // from the histogram (k_scatter then needs no atomics); nullptr: k_scatter
+  // takes places from bin_fill.
+  int32_t* fill;
 };
 
 // Grids with at least this many atoms per bin on average get chunk boxes.
