@@ -43,7 +43,6 @@ namespace {
 
 constexpr int kFThreads = 256;
 constexpr int kFWarps = kFThreads / 32;
-constexpr int kFMaskWords = 4096;  // hit-mask words kept per group
 constexpr int kFStage = 4096;      // output entries staged per window
 constexpr int kFJBits = 17;        // candidate offset bits of a stage entry
 
@@ -233,7 +232,7 @@ __global__ void __launch_bounds__(kFThreads, 4)
   FCell* cells = reinterpret_cast<FCell*>(fsm);
   uint32_t* pre = reinterpret_cast<uint32_t*>(fsm + fused_cells_bytes(n_cells));
   uint32_t* masks = pre + (n_cells + 1) * 32;
-  uint32_t* stage = masks + kFMaskWords;
+  uint32_t* stage = masks + o.mask_words;
   __shared__ float4 st_xy[kFWarps][16];
   __shared__ float2 st_z[kFWarps][16];
   __shared__ int2 st_w[kFWarps][16];
@@ -284,7 +283,7 @@ __global__ void __launch_bounds__(kFThreads, 4)
       for (int c = 0; c < n_cells; ++c) {
         const int32_t nc = cells[c].b1 - cells[c].b0;
         const int32_t words = ((nc + 31) >> 5) * 32;
-        if (acc + words <= kFMaskWords) {
+        if (acc + words <= o.mask_words) {
           cells[c].mbase = acc;
           acc += words;
         }
@@ -527,8 +526,8 @@ __global__ void __launch_bounds__(kFThreads, 4)
 
 }  // namespace
 
-size_t fused_smem_bytes(int32_t n_cells) {
-  return fused_cells_bytes(n_cells) + sizeof(uint32_t) * (((size_t)n_cells + 1) * 32 + kFMaskWords +
+size_t fused_smem_bytes(int32_t n_cells, int32_t mask_words) {
+  return fused_cells_bytes(n_cells) + sizeof(uint32_t) * (((size_t)n_cells + 1) * 32 + mask_words +
                                                            kFStage);
 }
 
@@ -557,7 +556,7 @@ void launch_move_dst(int64_t* src, const int64_t* dst, const int64_t* total, int
 
 void launch_pair_fused(const GridParams& g, const GridBuffers& b, int32_t n_cells,
                        const GuardBand& band, const FusedOut& o, cudaStream_t s) {
-  const size_t smem = fused_smem_bytes(n_cells);
+  const size_t smem = fused_smem_bytes(n_cells, o.mask_words);
   ensure_smem_attr((const void*)k_pair_fused, (int)smem);
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);

@@ -188,6 +188,12 @@ FusedOut fused_targets(Ctx& c, const SystemPlan& sp, int64_t capacity) {
   o.total = sp.fused_total;
   o.spin_limit = kFusedSpinLimit;
   o.withhold = -1;
+  {
+    const double per_bin = (double)sp.n / (double)std::max<int64_t>(sp.grid.total_bins, 1);
+    const int64_t chunks = (int64_t)std::ceil(1.5 * per_bin / 32.0);
+    const int64_t want = stencil_cells_of(sp.grid) * std::max<int64_t>(chunks, 1) * 32;
+    o.mask_words = (int32_t)std::min<int64_t>(std::max<int64_t>(want, kFusedMaskMin), kFusedMaskMax);
+  }
   int32_t tile = 0, spins = 0;
   if (take_scan_stall(&tile, &spins)) {  // failure-detection hook
     o.withhold = tile;

@@ -175,9 +175,13 @@ constexpr int64_t kPairMaxCells = 1024;
 // Needs the groups in canonical order (GridBuffers::group_start set for the
 // build) and at most kFusedMaxCells stencil cells.
 constexpr int32_t kFusedMaxCells = 125;
-// Grids with more atoms per bin than this keep the three-launch pipeline
-// (their hit masks would not fit in shared memory).
-constexpr double kFusedMaxPerBin = 64.0;
+// Grids with more atoms per bin than this keep the three-launch pipeline.
+constexpr double kFusedMaxPerBin = 512.0;
+// Hit-mask words a group keeps in shared memory: enough for every stencil
+// cell at 1.5 x the mean bin occupancy, within these bounds (cells beyond
+// the budget recompute their tests when the group writes).
+constexpr int32_t kFusedMaskMin = 4096;
+constexpr int32_t kFusedMaskMax = 12288;
 struct FusedOut {
   int64_t* src;       // [capacity] sources
   int64_t* dst;       // [capacity] destinations (a separate array)
@@ -187,11 +191,12 @@ struct FusedOut {
   int64_t* total;     // receives M
   int32_t spin_limit; // polls of one look-back wait before it gives up
   int32_t withhold;   // failure-detection hook: this group never publishes (-1: none)
+  int32_t mask_words; // hit-mask words per group in shared memory
 };
 __host__ __device__ inline size_t fused_cells_bytes(int32_t n_cells) {
   return ((size_t)88 * (size_t)n_cells + 15) & ~(size_t)15;
 }
-size_t fused_smem_bytes(int32_t n_cells);
+size_t fused_smem_bytes(int32_t n_cells, int32_t mask_words);
 // Moves the M destinations of the fused kernel behind the M sources (reads
 // M from *total; nothing when M > capacity).
 void launch_move_dst(int64_t* src, const int64_t* dst, const int64_t* total, int64_t capacity,
