@@ -711,46 +711,33 @@ __global__ void __launch_bounds__(256)
       yi = pi[1];
       zi = pi[2];
     }
-    // Four records at a time: their candidate gathers are in flight together
-    // before any of their stores.
-    for (int r0 = 0; r0 < hdr.z; r0 += 4) {
-      uint32_t mask[4], psh[4];
-      int32_t j0[4];
-      SlotMeta mj[4];
+    for (int r = 0; r < hdr.z; ++r) {
+      const uint32_t mask = __shfl_sync(0xffffffffu, my_mask, r);
+      const int32_t j0 = (int32_t)__shfl_sync(0xffffffffu, my_j, r);
+      const uint32_t psh = __shfl_sync(0xffffffffu, my_sh, r);
+      if ((mask >> lane) & 1u) {
+        const SlotMeta mj = rb.meta[slot + j0 + lane];
+        int32_t s[3];
+        if (method == 1) {
+          const double* pj = pos + 3 * (start + mj.orig);
+          double df[3];
+          matvec(P->g.hinv, dsub(pj[0], xi), dsub(pj[1], yi), dsub(pj[2], zi), df);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int r = r0 + u < 32 ? r0 + u : 31;
-        mask[u] = __shfl_sync(0xffffffffu, my_mask, r);
-        j0[u] = (int32_t)__shfl_sync(0xffffffffu, my_j, r);
-        psh[u] = __shfl_sync(0xffffffffu, my_sh, r);
-        if (r0 + u >= hdr.z) mask[u] = 0u;
-        if ((mask[u] >> lane) & 1u) mj[u] = rb.meta[slot + j0[u] + lane];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if ((mask[u] >> lane) & 1u) {
-          int32_t s[3];
-          if (method == 1) {
-            const double* pj = pos + 3 * (start + mj[u].orig);
-            double df[3];
-            matvec(P->g.hinv, dsub(pj[0], xi), dsub(pj[1], yi), dsub(pj[2], zi), df);
-#pragma unroll
-            for (int a = 0; a < 3; ++a) s[a] = sat_i32(P->pbc[a] ? -round(df[a]) : 0.0);
-          } else {
-            s[0] = (mj[u].sx - mi.sx) + ((int32_t)(psh[u] << 22) >> 22);
-            s[1] = (mj[u].sy - mi.sy) + ((int32_t)(psh[u] << 12) >> 22);
-            s[2] = (mj[u].sz - mi.sz) + ((int32_t)(psh[u] << 2) >> 22);
-          }
-          const int64_t e = cur + __popc(mask[u] & lanemask_lt());
-          src[e] = (int64_t)mi.orig + idx_off;
-          dst[e] = (int64_t)mj[u].orig + idx_off;
-          int32_t* sp = t.sh[0] + 3 * e;
-          sp[0] = s[0];
-          sp[1] = s[1];
-          sp[2] = s[2];
+          for (int a = 0; a < 3; ++a) s[a] = sat_i32(P->pbc[a] ? -round(df[a]) : 0.0);
+        } else {
+          s[0] = (mj.sx - mi.sx) + ((int32_t)(psh << 22) >> 22);
+          s[1] = (mj.sy - mi.sy) + ((int32_t)(psh << 12) >> 22);
+          s[2] = (mj.sz - mi.sz) + ((int32_t)(psh << 2) >> 22);
         }
-        cur += __popc(mask[u]);
+        const int64_t e = cur + __popc(mask & lanemask_lt());
+        src[e] = (int64_t)mi.orig + idx_off;
+        dst[e] = (int64_t)mj.orig + idx_off;
+        int32_t* sp = t.sh[0] + 3 * e;
+        sp[0] = s[0];
+        sp[1] = s[1];
+        sp[2] = s[2];
       }
+      cur += __popc(mask);
     }
   }
 }

@@ -175,8 +175,10 @@ constexpr int64_t kPairMaxCells = 1024;
 // Needs the groups in canonical order (GridBuffers::group_start set for the
 // build) and at most kFusedMaxCells stencil cells.
 constexpr int32_t kFusedMaxCells = 125;
-// Grids with more atoms per bin than this keep the three-launch pipeline.
-constexpr double kFusedMaxPerBin = 512.0;
+// Grids with more atoms per bin than this keep the three-launch pipeline
+// (measured at 370 atoms per bin, rc 14 on the cluster liquid: one launch
+// 326 us against 189 us for count + scan + emit).
+constexpr double kFusedMaxPerBin = 64.0;
 // Hit-mask words a group keeps in shared memory: enough for every stencil
 // cell at 1.5 x the mean bin occupancy, within these bounds (cells beyond
 // the budget recompute their tests when the group writes).
