@@ -59,6 +59,17 @@ __device__ __forceinline__ void f_store(uint64_t* p, uint64_t v) {
   *reinterpret_cast<volatile uint64_t*>(p) = v;
 }
 
+// {M, error word} to the host-mapped report, then its ready word.
+__device__ __forceinline__ void f_report(const FusedOut& o, int64_t m, int64_t err) {
+  if (!o.report) return;
+  __threadfence();
+  volatile int64_t* r = o.report;
+  r[1] = m;
+  r[2] = err;
+  __threadfence_system();
+  r[0] = 1;
+}
+
 struct FCell {
   double off[3];   // FP64 image offset (reference order)
   double cs[3];    // bin centre + offset: the prune test's target
@@ -519,9 +530,23 @@ __global__ void __launch_bounds__(kFThreads, 4)
       }
     }
     __syncthreads();
+    // One thread releases the group's writes (ordered before it by the
+    // barrier) with the completion count; the last group to complete reports.
+    if (tid == 0) {
+      __threadfence();
+      if (atomicAdd(o.done, 1ull) == (unsigned long long)n_groups - 1ull) {
+        __threadfence();
+        const int64_t m = *reinterpret_cast<volatile int64_t*>(o.total);
+        const int64_t err = (int64_t)f_load(&o.state[1]);
+        f_report(o, m, err);
+      }
+    }
   }
   // No groups at all: the list is empty.
-  if (n_groups == 0 && blockIdx.x == 0 && tid == 0) *o.total = 0;
+  if (n_groups == 0 && blockIdx.x == 0 && tid == 0) {
+    *o.total = 0;
+    f_report(o, 0, 0);
+  }
 }
 
 }  // namespace

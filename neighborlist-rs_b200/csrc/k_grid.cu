@@ -199,6 +199,113 @@ __device__ void smem_bitonic(uint64_t* k, int32_t* v, int cnt) {
   }
 }
 
+// Slot p of the sorted order holds atom idx: wrapped position, wrap shifts,
+// original index and, for the pair-task searches (p32 set), the packed FP32
+// position in its bin's frame, the bin and the irregular flag.  Returns the
+// packed position and the bin's index (zero without p32).
+struct SlotOut {
+  float4 q;
+  int32_t lin;
+};
+__device__ __forceinline__ SlotOut store_slot(const GridParams& g, const double* __restrict__ pos,
+                                             int64_t p, int32_t idx, double* __restrict__ px,
+                                             double* __restrict__ py, double* __restrict__ pz,
+                                             SlotMeta* __restrict__ meta,
+                                             float4* __restrict__ p32, int32_t* __restrict__ sbin,
+                                             int32_t* __restrict__ irr_list,
+                                             uint8_t* __restrict__ irr,
+                                             int32_t* __restrict__ counters) {
+  const AtomWrap w = wrap_atom(g, pos[3 * (int64_t)idx], pos[3 * (int64_t)idx + 1],
+                               pos[3 * (int64_t)idx + 2]);
+  px[p] = w.wx;
+  py[p] = w.wy;
+  pz[p] = w.wz;
+  SlotMeta mt;
+  mt.sx = w.s[0];
+  mt.sy = w.s[1];
+  mt.sz = w.s[2];
+  mt.orig = idx;
+  meta[p] = mt;
+  SlotOut so;
+  so.q = make_float4(0.f, 0.f, 0.f, 0.f);
+  so.lin = 0;
+  if (p32) {
+    // Bin centre of the stored bin (same expression as the prune test's
+    // target centre, src/search.rs:493-497).
+    double c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double t = dadd(g.origin[k], dmul(g.basis[0][k], (double)w.bin[0]));
+      t = dadd(t, dmul(g.basis[1][k], (double)w.bin[1]));
+      c[k] = dadd(t, dmul(g.basis[2][k], (double)w.bin[2]));
+    }
+    so.q = make_float4(__double2float_rn(dsub(w.wx, c[0])), __double2float_rn(dsub(w.wy, c[1])),
+                       __double2float_rn(dsub(w.wz, c[2])), __int_as_float(idx));
+    p32[p] = so.q;
+    so.lin = w.bin[0] + g.nb[0] * (w.bin[1] + g.nb[1] * w.bin[2]);
+    sbin[p] = so.lin;
+    // Home stencil centre, recomputed from the wrapped position exactly as
+    // the search does (src/search.rs:454-457).
+    double fi[3];
+    matvec(g.hinv, w.wx, w.wy, w.wz, fi);
+    bool same = true;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const int32_t v = sat_i32(dmul(fi[a], (double)g.nb[a]));
+      const int32_t hb = v < g.nb[a] - 1 ? v : g.nb[a] - 1;
+      same = same && hb == w.bin[a];
+    }
+    irr[p] = same ? 0 : 1;
+    if (!same) irr_list[atomicAdd(&counters[1], 1)] = (int32_t)p;
+  }
+  return so;
+}
+
+// Bounding box of one 32-slot chunk held by a warp, one slot per lane
+// (`valid`: the lane holds a slot); lane 0 stores it at box[0..1].
+__device__ __forceinline__ void warp_box(float4 q, bool valid, float4* __restrict__ box) {
+  float4 lo = q, hi = q;
+  if (!valid) {
+    lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+    hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = fminf(lo.x, __shfl_xor_sync(0xffffffffu, lo.x, o));
+    lo.y = fminf(lo.y, __shfl_xor_sync(0xffffffffu, lo.y, o));
+    lo.z = fminf(lo.z, __shfl_xor_sync(0xffffffffu, lo.z, o));
+    hi.x = fmaxf(hi.x, __shfl_xor_sync(0xffffffffu, hi.x, o));
+    hi.y = fmaxf(hi.y, __shfl_xor_sync(0xffffffffu, hi.y, o));
+    hi.z = fmaxf(hi.z, __shfl_xor_sync(0xffffffffu, hi.z, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    box[0] = make_float4(lo.x, lo.y, lo.z, 0.f);
+    box[1] = make_float4(hi.x, hi.y, hi.z, 0.f);
+  }
+}
+
+// The group records of the bin of rank r (slots [s, e), bin index lin), at
+// their canonical place when the group starts are known (bins in rank order,
+// 32-atom runs in slot order), else where a counter puts them.
+__device__ __forceinline__ void store_groups(const GridParams& g, int64_t r, int64_t s, int64_t e,
+                                             int32_t lin, GroupRec* __restrict__ groups,
+                                             int32_t* __restrict__ counters,
+                                             const int32_t* __restrict__ group_start) {
+  const int ng = (int)((e - s + 31) / 32);
+  const int placed = atomicAdd(&counters[0], ng);
+  const int base = group_start ? group_start[r] : placed;
+  GroupRec gr;
+  gr.end = (int32_t)e;
+  gr.lin = lin;
+  gr.bx = lin % g.nb[0];
+  gr.by = (lin / g.nb[0]) % g.nb[1];
+  gr.bz = lin / (g.nb[0] * g.nb[1]);
+  for (int k = 0; k < ng; ++k) {
+    gr.first = (int32_t)(s + 32 * k);
+    groups[base + k] = gr;
+  }
+}
+
 __global__ void __launch_bounds__(kSortThreads)
     k_binsort(GridParams g, const double* __restrict__ pos, const int64_t* __restrict__ bin_start,
               uint64_t* __restrict__ skey, int32_t* __restrict__ sidx,
@@ -220,39 +327,44 @@ __global__ void __launch_bounds__(kSortThreads)
   const int32_t* final_idx = sidx;
   if (cnt <= 32) {
     // Bins of at most 32 atoms: one warp sorts them in registers (bitonic
-    // network over the lanes), no shared memory or block barriers.
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
-      uint64_t k = ~0ull;
-      int32_t v = 0x7fffffff;
-      if (lane < cnt) {
-        k = skey[s + lane];
-        v = sidx[s + lane];
-      }
-      for (int size = 2; size <= 32; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-          const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, stride);
-          const int32_t ov = __shfl_xor_sync(0xffffffffu, v, stride);
-          const bool up = (lane & size) == 0;
-          const bool lower = (lane & stride) == 0;
-          // The lower lane of an ascending pair keeps the smaller element.
-          const bool other_less = pair_less(ok, ov, k, v);
-          const bool take = (lower == up) ? other_less : pair_less(k, v, ok, ov);
-          if (take) {
-            k = ok;
-            v = ov;
-          }
+    // network over the lanes) and writes every output of the bin from
+    // registers (slots, chunk box, group record): no shared memory, no block
+    // barrier, no re-read of the sorted order.
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    uint64_t k = ~0ull;
+    int32_t v = 0x7fffffff;
+    if (lane < cnt) {
+      k = skey[s + lane];
+      v = sidx[s + lane];
+    }
+    for (int size = 2; size <= 32; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, stride);
+        const int32_t ov = __shfl_xor_sync(0xffffffffu, v, stride);
+        const bool up = (lane & size) == 0;
+        const bool lower = (lane & stride) == 0;
+        // The lower lane of an ascending pair keeps the smaller element.
+        const bool other_less = pair_less(ok, ov, k, v);
+        const bool take = (lower == up) ? other_less : pair_less(k, v, ok, ov);
+        if (take) {
+          k = ok;
+          v = ov;
         }
       }
-      if (lane < cnt) {
-        skey[s + lane] = k;
-        sidx[s + lane] = v;
-      }
     }
-    __syncthreads();
+    SlotOut so;
+    so.q = make_float4(0.f, 0.f, 0.f, 0.f);
+    so.lin = 0;
+    if (lane < cnt)
+      so = store_slot(g, pos, s + lane, v, px, py, pz, meta, p32, sbin, irr_list, irr, counters);
+    if (!p32) return;
+    if (cbox) warp_box(so.q, lane < cnt, cbox + 2 * s);
+    if (lane == 0) store_groups(g, r, s, e, so.lin, groups, counters, group_start);
+    return;
   }
   // Sort chunks of kSortCap in shared memory (the whole bin when it fits).
-  for (int64_t c0 = 0; cnt > 32 && c0 < cnt; c0 += kSortCap) {
+  for (int64_t c0 = 0; c0 < cnt; c0 += kSortCap) {
     const int m = (int)(cnt - c0 < kSortCap ? cnt - c0 : kSortCap);
     for (int i = threadIdx.x; i < m; i += blockDim.x) {
       sk[i] = skey[s + c0 + i];
@@ -307,88 +419,22 @@ __global__ void __launch_bounds__(kSortThreads)
     final_idx = av - s;
   }
   // Gather the sorted slots: wrapped positions, wrap shifts, original index.
-  for (int64_t p = s + threadIdx.x; p < e; p += blockDim.x) {
-    const int32_t idx = final_idx[p];
-    const AtomWrap w = wrap_atom(g, pos[3 * (int64_t)idx], pos[3 * (int64_t)idx + 1],
-                                 pos[3 * (int64_t)idx + 2]);
-    px[p] = w.wx;
-    py[p] = w.wy;
-    pz[p] = w.wz;
-    SlotMeta mt;
-    mt.sx = w.s[0];
-    mt.sy = w.s[1];
-    mt.sz = w.s[2];
-    mt.orig = idx;
-    meta[p] = mt;
-    if (p32) {
-      // Bin centre of the stored bin (same expression as the prune test's
-      // target centre, src/search.rs:493-497).
-      double c[3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        double t = dadd(g.origin[k], dmul(g.basis[0][k], (double)w.bin[0]));
-        t = dadd(t, dmul(g.basis[1][k], (double)w.bin[1]));
-        c[k] = dadd(t, dmul(g.basis[2][k], (double)w.bin[2]));
-      }
-      p32[p] = make_float4(__double2float_rn(dsub(w.wx, c[0])), __double2float_rn(dsub(w.wy, c[1])),
-                           __double2float_rn(dsub(w.wz, c[2])), __int_as_float(idx));
-      sbin[p] = w.bin[0] + g.nb[0] * (w.bin[1] + g.nb[1] * w.bin[2]);
-      // Home stencil centre, recomputed from the wrapped position exactly as
-      // the search does (src/search.rs:454-457).
-      double fi[3];
-      matvec(g.hinv, w.wx, w.wy, w.wz, fi);
-      bool same = true;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int32_t v = sat_i32(dmul(fi[a], (double)g.nb[a]));
-        const int32_t hb = v < g.nb[a] - 1 ? v : g.nb[a] - 1;
-        same = same && hb == w.bin[a];
-      }
-      irr[p] = same ? 0 : 1;
-      if (!same) irr_list[atomicAdd(&counters[1], 1)] = (int32_t)p;
-    }
+  // Each warp pass covers one 32-slot chunk (offsets from s are multiples of
+  // 32), whose box it reduces in registers.
+  const int lane = threadIdx.x & 31;
+  int32_t lin0 = 0;
+  for (int64_t p0 = s + (threadIdx.x & ~31); p0 < e; p0 += blockDim.x) {
+    const int64_t p = p0 + lane;
+    SlotOut so;
+    so.q = make_float4(0.f, 0.f, 0.f, 0.f);
+    so.lin = 0;
+    if (p < e)
+      so = store_slot(g, pos, p, final_idx[p], px, py, pz, meta, p32, sbin, irr_list, irr,
+                      counters);
+    if (p == s) lin0 = so.lin;
+    if (p32 && cbox) warp_box(so.q, p < e, cbox + 2 * p0);
   }
-  if (p32 && cbox) {
-    // Bounding box of each 32-atom chunk (the p32 values just written by this
-    // block's threads).
-    __syncthreads();
-    const int ng = (int)((cnt + 31) / 32);
-    for (int k = threadIdx.x; k < ng; k += blockDim.x) {
-      const int64_t c0 = s + 32 * (int64_t)k;
-      const int64_t c1 = c0 + 32 < e ? c0 + 32 : e;
-      float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
-      float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
-      for (int64_t p = c0; p < c1; ++p) {
-        const float4 a = p32[p];
-        lo.x = fminf(lo.x, a.x);
-        lo.y = fminf(lo.y, a.y);
-        lo.z = fminf(lo.z, a.z);
-        hi.x = fmaxf(hi.x, a.x);
-        hi.y = fmaxf(hi.y, a.y);
-        hi.z = fmaxf(hi.z, a.z);
-      }
-      cbox[2 * c0] = lo;
-      cbox[2 * c0 + 1] = hi;
-    }
-  }
-  if (p32 && threadIdx.x == 0) {
-    const int ng = (int)((cnt + 31) / 32);
-    // (canonical position when the group starts are known: bins in rank
-    // order, 32-atom runs in slot order)
-    const int placed = atomicAdd(&counters[0], ng);
-    const int base = group_start ? group_start[r] : placed;
-    const int32_t lin = sbin[s];
-    GroupRec gr;
-    gr.end = (int32_t)e;
-    gr.lin = lin;
-    gr.bx = lin % g.nb[0];
-    gr.by = (lin / g.nb[0]) % g.nb[1];
-    gr.bz = lin / (g.nb[0] * g.nb[1]);
-    for (int k = 0; k < ng; ++k) {
-      gr.first = (int32_t)(s + 32 * k);
-      groups[base + k] = gr;
-    }
-  }
+  if (p32 && threadIdx.x == 0) store_groups(g, r, s, e, lin0, groups, counters, group_start);
 }
 
 constexpr int kBoundsThreads = 1024;

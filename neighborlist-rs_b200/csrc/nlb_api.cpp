@@ -419,6 +419,8 @@ void release_thread_ctx() {
       if (ev) cudaEventDestroy(ev);
     tune_release(*c);
     if (c->h_small) cudaFreeHost(c->h_small);
+    if (c->h_report) cudaFreeHost(c->h_report);
+    if (c->early_ev) cudaEventDestroy(c->early_ev);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     cudaSetDevice(prev);
     delete c;
@@ -442,10 +444,22 @@ Status get_ctx(Ctx** out) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
     e = cudaHostAlloc((void**)&c->h_small, sizeof(int64_t) * kSmallHost, cudaHostAllocDefault);
     if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc");
+    e = cudaHostAlloc((void**)&c->h_report, sizeof(int64_t) * 8, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&c->d_report, c->h_report, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaHostAlloc (mapped)");
+    e = cudaEventCreateWithFlags(&c->early_ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
     for (int i = 0; i < 6; ++i) cudaEventCreate(&c->ev[i]);
     ctxs[dev] = c;
   }
   c->stream = tl_user_stream ? tl_user_stream : c->own_stream;
+  if (c->early_stream && c->early_stream != c->stream) {
+    // The last call returned early on another stream: this stream's work
+    // follows it.
+    e = cudaStreamWaitEvent(c->stream, c->early_ev, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+    c->early_stream = nullptr;
+  }
   if (tl_profile != c->prof) {
     c->prof = tl_profile;
     c->prof_pending_count = c->prof_pending_emit = false;

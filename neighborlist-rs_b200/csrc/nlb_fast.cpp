@@ -122,7 +122,7 @@ Status prepare_fast(Ctx& c, SystemPlan& sp, int64_t capacity, int64_t mask_cap) 
   // (Fused launch: its ticket, error and look-back words and its total take
   // the scan state's place.)
   const int64_t max_groups = n / 32 + std::min<int64_t>(n, nb) + 1;
-  sp.fused_words = 2 + max_groups + 1;
+  sp.fused_words = 2 + max_groups + 2;  // + total, completion count
   sp.zeroed_words = 2 * (size_t)nb + 6 +
                     2 * (size_t)(sp.fused ? sp.fused_words : scan_tmp_elems(row));
   int32_t* zeroed = slot<int32_t>(c, kSlotBinCount, sp.zeroed_words);
@@ -186,6 +186,8 @@ FusedOut fused_targets(Ctx& c, const SystemPlan& sp, int64_t capacity) {
   o.capacity = capacity;
   o.state = sp.fused_state;
   o.total = sp.fused_total;
+  o.done = reinterpret_cast<unsigned long long*>(sp.fused_total + 1);
+  o.report = c.prof ? nullptr : c.d_report;
   o.spin_limit = kFusedSpinLimit;
   o.withhold = -1;
   {
@@ -248,8 +250,30 @@ void issue_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t capacity,
   c.mark(5);
 }
 
+// Waits until the launch just issued has filled the host-mapped report
+// (c.h_report[0] = 1), polling the stream now and then: a stream that failed,
+// or ended without a report, ends the wait with an error.
+Status wait_report(Ctx& c) {
+  volatile int64_t* r = c.h_report;
+  for (uint32_t k = 1; r[0] == 0; ++k) {
+    if ((k & 127) != 0) continue;
+    const cudaError_t q = cudaStreamQuery(c.stream);
+    if (q == cudaErrorNotReady) continue;
+    if (q != cudaSuccess) return cuda_fail(q, "neighbour-list pipeline");
+    if (r[0] == 0) return fail(NLB_ERR_CUDA, "the one-launch search ended without its report");
+  }
+  std::atomic_thread_fence(std::memory_order_acquire);
+  return Status{NLB_OK};
+}
+
 // Runs the fast pipeline for a planned single-cutoff cell-list system and
 // leaves M edges in sp.out_src ([src | dst]) / sp.out_sh.
+//
+// The one-launch search reports M through host-mapped memory as soon as its
+// last group is done.  On a caller's stream the call then returns at once:
+// the remaining work (the move of the destinations) is queued on that stream
+// ahead of anything the caller queues there.  On the library's own stream it
+// also waits for that work.
 Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, bool contiguous) {
   FastState& fs = state_for(c);
   const int64_t n_cells = stencil_cells_of(sp.grid);
@@ -285,6 +309,9 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, boo
   key.prof = c.prof ? 1 : 0;
   key.fused = sp.fused ? 1 : 0;
   key.contiguous = contiguous ? 1 : 0;
+
+  const bool report = sp.fused && !c.prof;
+  if (report) c.h_report[0] = 0;
 
   // (An armed failure-detection hook must reach a directly launched scan,
   // never a captured or replayed one.)
@@ -334,6 +361,30 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, boo
   fs.key = key;
   fs.have_key = true;
   for (int a = 0; a < 3; ++a) c.rank_nb[a] = sp.grid.nb[a];
+
+  if (report) {
+    Status rs = wait_report(c);
+    if (!rs.ok()) return rs;
+    const volatile int64_t* r = c.h_report;
+    const int64_t m = r[1];
+    if (r[2] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+    if (m <= capacity) {
+      if (c.stream == c.own_stream) {
+        const cudaError_t e = cudaStreamSynchronize(c.stream);
+        if (e != cudaSuccess) return cuda_fail(e, "neighbour-list pipeline");
+      } else {
+        const cudaError_t e = cudaEventRecord(c.early_ev, c.stream);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+        c.early_stream = c.stream;
+      }
+      sp.out_dst = contiguous ? sp.out_src + m : static_cast<int64_t*>(c.bufs[kSlotOutDst].p);
+      fs.last_m = m;
+      fs.last_mask_words = 0;
+      *m_out = m;
+      return Status{NLB_OK};
+    }
+    // (M above the capacity: the synchronous path below grows the arrays.)
+  }
 
   // One synchronisation: total edges and the scan's wait-error word.
   cudaError_t e = cudaMemcpyAsync(c.h_small, sp.fused ? sp.fused_total : sp.offs + sp.row,

@@ -82,6 +82,16 @@ struct Ctx {
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;  // active stream: the caller's (nlb_set_stream) or own_stream
   int64_t* h_small = nullptr;     // pinned scratch for small device->host reads
+  // Host-mapped pinned record a kernel fills when the edge count is known:
+  // [0] ready (1), [1] M, [2] error word (h_report: host view, d_report:
+  // device view).
+  int64_t* h_report = nullptr;
+  int64_t* d_report = nullptr;
+  // A call on a caller's stream may return before its last kernels end (the
+  // results are complete in that stream's order).  early_ev marks the end of
+  // that work; a later call on another stream waits for it on the device.
+  cudaEvent_t early_ev = nullptr;
+  cudaStream_t early_stream = nullptr;
   Buf bufs[kSlotCount];
   // Batched outputs: [src, dst, shift] per cutoff, grow-only and kept across
   // calls (results are appended run by run, so growth preserves contents).

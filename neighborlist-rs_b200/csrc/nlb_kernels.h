@@ -191,6 +191,12 @@ struct FusedOut {
   int64_t capacity;   // a group whose block does not fit writes nothing
   uint64_t* state;    // zeroed: [0] group ticket, [1] error word, [2 + g] group g's look-back word
   int64_t* total;     // receives M
+  // Zeroed completion count of the groups; the group that completes it
+  // copies {M, error word} into `report` (host-mapped pinned memory, may be
+  // null) and then sets report[0] = 1, so the host learns M without waiting
+  // for the launch (or the ones queued after it) to end.
+  unsigned long long* done;
+  int64_t* report;
   int32_t spin_limit; // polls of one look-back wait before it gives up
   int32_t withhold;   // failure-detection hook: this group never publishes (-1: none)
   int32_t mask_words; // hit-mask words per group in shared memory

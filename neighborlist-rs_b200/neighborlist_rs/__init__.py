@@ -169,7 +169,7 @@ class PyCell:
     all periodic.  ``from_ase`` transposes an ASE cell (rows = vectors).
     """
 
-    __slots__ = ("_h9", "_pbc")
+    __slots__ = ("_h9", "_pbc", "_args")
 
     def __init__(self, h, pbc=None):
         rows = [list(r) for r in h] if not isinstance(h, (str, bytes)) else []
@@ -182,14 +182,16 @@ class PyCell:
         if len(p) != 3:
             raise ValueError("pbc must have 3 entries")
         self._pbc = np.ascontiguousarray(np.array(p, dtype=np.uint8))
-        _check(_lib.nlb_cell_check(self._h9.ctypes.data_as(_dp)))
+        # ctypes pointers made once (each data_as costs ~2 us per call)
+        self._args = (self._h9.ctypes.data_as(_dp), self._pbc.ctypes.data_as(_u8p))
+        _check(_lib.nlb_cell_check(self._args[0]))
 
     def wrap(self, pos):
         p = np.ascontiguousarray(np.array([float(x) for x in pos], dtype=np.float64))
         if p.shape != (3,):
             raise ValueError("pos must have 3 entries")
         out = np.zeros(3, np.float64)
-        _check(_lib.nlb_cell_wrap(self._h9.ctypes.data_as(_dp), self._pbc.ctypes.data_as(_u8p),
+        _check(_lib.nlb_cell_wrap(self._args[0], self._args[1],
                                   p.ctypes.data_as(_dp), out.ctypes.data_as(_dp)))
         return [float(v) for v in out]
 
@@ -213,7 +215,7 @@ def _cell_args(cell):
         return None, None
     if not isinstance(cell, PyCell):
         raise TypeError("cell must be a PyCell or None")
-    return cell._h9.ctypes.data_as(_dp), cell._pbc.ctypes.data_as(_u8p)
+    return cell._args
 
 
 def build_neighborlists(cell, positions, cutoff, parallel=True):
