@@ -8,10 +8,14 @@
 //   k_prep       : per atom: fraction, wrap, Morton key, bin rank, bin histogram.
 //   (scan)       : bin histogram -> bin starts.
 //   k_scatter    : atoms -> bin segments (arbitrary order inside a segment).
-//   k_binsort    : one CTA per bin sorts its (key, index) pairs -- bitonic in
+//   k_place      : every atom to its slot (wrapped positions, wrap shifts,
+//                  original indices, packed FP32 positions, group records):
+//                  in bins of at most kRankSortMax atoms one thread per atom
+//                  counts the bin's (key, index) pairs below its own (rank
+//                  sort); larger bins are sorted by one CTA each -- bitonic in
 //                  shared memory up to kSortCap, merge path through global
-//                  scratch above it -- and gathers the sorted SoA arrays
-//                  (wrapped positions, wrap shifts, original indices).
+//                  scratch above it.
+//   k_chunk_box  : bounding box of each 32-atom chunk (dense grids only).
 #include "nlb_kernels.h"
 
 namespace nlb {
@@ -20,6 +24,7 @@ namespace {
 
 constexpr int kSortThreads = 128;
 constexpr int kSortCap = 2048;  // elements sorted entirely in shared memory
+constexpr int64_t kRankSortMax = 512;  // bins up to this size: rank placement
 
 // Grid points p (0 <= p_a < nb_a) whose Morton code is smaller than that of c.
 __device__ int64_t morton_rank(const int32_t c[3], const int32_t nb[3]) {
@@ -306,63 +311,23 @@ __device__ __forceinline__ void store_groups(const GridParams& g, int64_t r, int
   }
 }
 
-__global__ void __launch_bounds__(kSortThreads)
-    k_binsort(GridParams g, const double* __restrict__ pos, const int64_t* __restrict__ bin_start,
-              uint64_t* __restrict__ skey, int32_t* __restrict__ sidx,
-              uint64_t* __restrict__ skey2, int32_t* __restrict__ sidx2,
-              double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz,
-              SlotMeta* __restrict__ meta, float4* __restrict__ p32, int32_t* __restrict__ sbin,
-              GroupRec* __restrict__ groups, int32_t* __restrict__ irr_list,
-              uint8_t* __restrict__ irr, int32_t* __restrict__ counters,
-              float4* __restrict__ cbox, const int32_t* __restrict__ group_start) {
-  __shared__ uint64_t sk[kSortCap];
-  __shared__ int32_t sv[kSortCap];
-  pdl_wait();
-  const int64_t r = blockIdx.x;
+// Bins of more than kRankSortMax atoms: one CTA sorts the bin of rank r --
+// bitonic in shared memory up to kSortCap, merge path through global scratch
+// above it -- and gathers its slots.
+__device__ void sort_bin(const GridParams& g, const double* __restrict__ pos, int64_t r,
+                         const int64_t* __restrict__ bin_start, uint64_t* __restrict__ skey,
+                         int32_t* __restrict__ sidx, uint64_t* __restrict__ skey2,
+                         int32_t* __restrict__ sidx2, double* __restrict__ px,
+                         double* __restrict__ py, double* __restrict__ pz,
+                         SlotMeta* __restrict__ meta, float4* __restrict__ p32,
+                         int32_t* __restrict__ sbin, GroupRec* __restrict__ groups,
+                         int32_t* __restrict__ irr_list, uint8_t* __restrict__ irr,
+                         int32_t* __restrict__ counters, float4* __restrict__ cbox,
+                         const int32_t* __restrict__ group_start, uint64_t* sk, int32_t* sv) {
   const int64_t s = bin_start[r];
   const int64_t e = bin_start[r + 1];
   const int64_t cnt = e - s;
-  if (cnt == 0) return;
-
   const int32_t* final_idx = sidx;
-  if (cnt <= 32) {
-    // Bins of at most 32 atoms: one warp sorts them in registers (bitonic
-    // network over the lanes) and writes every output of the bin from
-    // registers (slots, chunk box, group record): no shared memory, no block
-    // barrier, no re-read of the sorted order.
-    if (threadIdx.x >= 32) return;
-    const int lane = threadIdx.x;
-    uint64_t k = ~0ull;
-    int32_t v = 0x7fffffff;
-    if (lane < cnt) {
-      k = skey[s + lane];
-      v = sidx[s + lane];
-    }
-    for (int size = 2; size <= 32; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        const uint64_t ok = __shfl_xor_sync(0xffffffffu, k, stride);
-        const int32_t ov = __shfl_xor_sync(0xffffffffu, v, stride);
-        const bool up = (lane & size) == 0;
-        const bool lower = (lane & stride) == 0;
-        // The lower lane of an ascending pair keeps the smaller element.
-        const bool other_less = pair_less(ok, ov, k, v);
-        const bool take = (lower == up) ? other_less : pair_less(k, v, ok, ov);
-        if (take) {
-          k = ok;
-          v = ov;
-        }
-      }
-    }
-    SlotOut so;
-    so.q = make_float4(0.f, 0.f, 0.f, 0.f);
-    so.lin = 0;
-    if (lane < cnt)
-      so = store_slot(g, pos, s + lane, v, px, py, pz, meta, p32, sbin, irr_list, irr, counters);
-    if (!p32) return;
-    if (cbox) warp_box(so.q, lane < cnt, cbox + 2 * s);
-    if (lane == 0) store_groups(g, r, s, e, so.lin, groups, counters, group_start);
-    return;
-  }
   // Sort chunks of kSortCap in shared memory (the whole bin when it fits).
   for (int64_t c0 = 0; c0 < cnt; c0 += kSortCap) {
     const int m = (int)(cnt - c0 < kSortCap ? cnt - c0 : kSortCap);
@@ -437,6 +402,66 @@ __global__ void __launch_bounds__(kSortThreads)
   if (p32 && threadIdx.x == 0) store_groups(g, r, s, e, lin0, groups, counters, group_start);
 }
 
+// Places every atom at its slot.  Blocks [0, atom_blocks): one thread per
+// entry p of the bin segments k_scatter wrote (arbitrary order inside a
+// segment); for bins of at most kRankSortMax atoms the atom's place in its
+// bin is the number of the bin's (key, index) pairs below its own (a rank
+// sort: the bin's pairs are read by each of its atoms, from L1), and the
+// thread writes the slot there directly; the atom placed first writes the
+// bin's group records.  Blocks from atom_blocks on: block atom_blocks + r
+// sorts bin r when it is larger (sort_bin).
+__global__ void __launch_bounds__(kSortThreads)
+    k_place(GridParams g, const double* __restrict__ pos, int64_t n,
+            const int32_t* __restrict__ rank, const int64_t* __restrict__ bin_start,
+            uint64_t* __restrict__ skey, int32_t* __restrict__ sidx,
+            uint64_t* __restrict__ skey2, int32_t* __restrict__ sidx2,
+            double* __restrict__ px, double* __restrict__ py, double* __restrict__ pz,
+            SlotMeta* __restrict__ meta, float4* __restrict__ p32, int32_t* __restrict__ sbin,
+            GroupRec* __restrict__ groups, int32_t* __restrict__ irr_list,
+            uint8_t* __restrict__ irr, int32_t* __restrict__ counters,
+            float4* __restrict__ cbox, const int32_t* __restrict__ group_start,
+            int32_t atom_blocks) {
+  __shared__ uint64_t sk[kSortCap];
+  __shared__ int32_t sv[kSortCap];
+  pdl_wait();
+  if ((int32_t)blockIdx.x >= atom_blocks) {
+    const int64_t r = (int64_t)blockIdx.x - atom_blocks;
+    if (bin_start[r + 1] - bin_start[r] <= kRankSortMax) return;
+    sort_bin(g, pos, r, bin_start, skey, sidx, skey2, sidx2, px, py, pz, meta, p32, sbin, groups,
+             irr_list, irr, counters, cbox, group_start, sk, sv);
+    return;
+  }
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const uint64_t k = skey[p];
+  const int32_t i = sidx[p];
+  const int32_t r = rank[i];
+  const int64_t s = bin_start[r], e = bin_start[r + 1];
+  if (e - s > kRankSortMax) return;
+  int32_t below = 0;
+  for (int64_t q = s; q < e; ++q) below += pair_less(__ldg(&skey[q]), __ldg(&sidx[q]), k, i) ? 1 : 0;
+  const SlotOut so = store_slot(g, pos, s + below, i, px, py, pz, meta, p32, sbin, irr_list, irr,
+                                counters);
+  if (p32 && below == 0) store_groups(g, r, s, e, so.lin, groups, counters, group_start);
+}
+
+// Bounding box of every 32-atom group's chunk (one warp per group).
+__global__ void k_chunk_box(const GroupRec* __restrict__ groups,
+                            const int32_t* __restrict__ counters, const float4* __restrict__ p32,
+                            float4* __restrict__ cbox) {
+  pdl_wait();
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t ng = counters[0];
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ng; t += nw) {
+    const GroupRec gr = groups[t];
+    const int32_t end = gr.end - gr.first < 32 ? gr.end : gr.first + 32;
+    const bool valid = gr.first + lane < end;
+    const float4 q = valid ? p32[gr.first + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    warp_box(q, valid, cbox + 2 * (int64_t)gr.first);
+  }
+}
+
 constexpr int kBoundsThreads = 1024;
 
 __global__ void __launch_bounds__(kBoundsThreads)
@@ -499,11 +524,20 @@ void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const 
   if (!fused) exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
   launch_pdl(k_scatter, dim3((unsigned)((n + T - 1) / T)), dim3(T), 0, s, b.key, b.rank, n,
              b.bin_start, b.bin_fill, b.skey, b.sidx, (const int32_t*)b.fill);
-  launch_pdl(k_binsort, dim3((unsigned)g.total_bins), dim3(kSortThreads), 0, s, g, pos,
-             b.bin_start, b.skey, b.sidx, b.skey2, b.sidx2, b.px, b.py, b.pz, b.meta, b.p32,
-             b.sbin, b.groups, b.irr_list, b.irr, b.counters, b.cbox,
-             fused ? b.group_start : nullptr);
+  const int32_t atom_blocks = (int32_t)((n + kSortThreads - 1) / kSortThreads);
+  launch_pdl(k_place, dim3((unsigned)(atom_blocks + g.total_bins)), dim3(kSortThreads), 0, s, g,
+             pos, n, (const int32_t*)b.rank, (const int64_t*)b.bin_start, b.skey, b.sidx, b.skey2,
+             b.sidx2, b.px, b.py, b.pz, b.meta, b.p32, b.sbin, b.groups, b.irr_list, b.irr,
+             b.counters, b.cbox, fused ? (const int32_t*)b.group_start : nullptr, atom_blocks);
   note_launches(3);
+  if (b.p32 && b.cbox) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    launch_pdl(k_chunk_box, dim3((unsigned)(2 * sms)), dim3(256), 0, s, (const GroupRec*)b.groups,
+               (const int32_t*)b.counters, (const float4*)b.p32, b.cbox);
+    note_launches(1);
+  }
 }
 
 }  // namespace nlb

@@ -221,6 +221,14 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? (K == 1 ? 3 : 1) : (K 
   int32_t* sw = reinterpret_cast<int32_t*>(stage_w[warp]);
   SlotMeta* smt = stage_m[warp];
   pdl_wait();
+  if (EMIT && t.report && blockIdx.x == 0 && threadIdx.x == 0) {
+    volatile int64_t* r = t.report;
+    r[1] = t.total_dev ? *t.total_dev : 0;
+    r[2] = (t.scan_error ? *t.scan_error : 0) | (t.grid_scan_error ? *t.grid_scan_error : 0);
+    r[3] = t.mask_top ? (int64_t)*t.mask_top : 0;
+    __threadfence_system();
+    r[0] = 1;
+  }
   int64_t* dst0 = EMIT ? t.dst[0] : nullptr;
   if (EMIT && t.scan_error && *t.scan_error != 0) return;  // offsets not valid
   if (EMIT && t.total_dev) {

@@ -211,7 +211,7 @@ void issue_fused(Ctx& c, SystemPlan& sp, int64_t capacity, bool contiguous) {
   if (contiguous) launch_move_dst(o.src, o.dst, o.total, capacity, c.stream);
 }
 
-EmitTargets fast_targets(const SystemPlan& sp, int64_t capacity) {
+EmitTargets fast_targets(const SystemPlan& sp, int64_t capacity, int64_t* report = nullptr) {
   EmitTargets t;
   std::memset(&t, 0, sizeof(t));
   t.src[0] = sp.out_src;
@@ -219,6 +219,10 @@ EmitTargets fast_targets(const SystemPlan& sp, int64_t capacity) {
   t.total_dev = sp.offs + sp.row;
   t.capacity = capacity;
   t.scan_error = sp.scan_state + 1;
+  t.report = report;
+  t.mask_top = sp.gb.mask_top;
+  // (grids too large for k_prep's own bin scan: the separate scan's error word)
+  t.grid_scan_error = sp.grid.total_bins > kFusedBinScanMax ? sp.gb.scan_tmp + 1 : nullptr;
   return t;
 }
 
@@ -246,7 +250,8 @@ void issue_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t capacity,
   exclusive_scan_u32_zeroed(sp.counts, sp.row, sp.offs, sp.scan_state, s);
   c.mark(3);
   c.mark(4);
-  launch_pair_emit(sp.grid, sp.gb, n, sp.band, sp.offs, fast_targets(sp, capacity), s);
+  launch_pair_emit(sp.grid, sp.gb, n, sp.band, sp.offs,
+                   fast_targets(sp, capacity, c.prof ? nullptr : c.d_report), s);
   c.mark(5);
 }
 
@@ -260,7 +265,7 @@ Status wait_report(Ctx& c) {
     const cudaError_t q = cudaStreamQuery(c.stream);
     if (q == cudaErrorNotReady) continue;
     if (q != cudaSuccess) return cuda_fail(q, "neighbour-list pipeline");
-    if (r[0] == 0) return fail(NLB_ERR_CUDA, "the one-launch search ended without its report");
+    if (r[0] == 0) return fail(NLB_ERR_CUDA, "the search ended without its report");
   }
   std::atomic_thread_fence(std::memory_order_acquire);
   return Status{NLB_OK};
@@ -269,11 +274,12 @@ Status wait_report(Ctx& c) {
 // Runs the fast pipeline for a planned single-cutoff cell-list system and
 // leaves M edges in sp.out_src ([src | dst]) / sp.out_sh.
 //
-// The one-launch search reports M through host-mapped memory as soon as its
-// last group is done.  On a caller's stream the call then returns at once:
-// the remaining work (the move of the destinations) is queued on that stream
-// ahead of anything the caller queues there.  On the library's own stream it
-// also waits for that work.
+// M reaches the host through host-mapped memory as soon as it is known: the
+// one-launch search reports it when its last group is done, the three-launch
+// pipeline when its emit pass starts.  On a caller's stream the call then
+// returns at once: the remaining work (the emit, or the move of the
+// destinations) is queued on that stream ahead of anything the caller queues
+// there.  On the library's own stream it also waits for that work.
 Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, bool contiguous) {
   FastState& fs = state_for(c);
   const int64_t n_cells = stencil_cells_of(sp.grid);
@@ -310,7 +316,7 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, boo
   key.fused = sp.fused ? 1 : 0;
   key.contiguous = contiguous ? 1 : 0;
 
-  const bool report = sp.fused && !c.prof;
+  const bool report = !c.prof;
   if (report) c.h_report[0] = 0;
 
   // (An armed failure-detection hook must reach a directly launched scan,
@@ -377,9 +383,10 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, boo
         if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
         c.early_stream = c.stream;
       }
-      sp.out_dst = contiguous ? sp.out_src + m : static_cast<int64_t*>(c.bufs[kSlotOutDst].p);
+      sp.out_dst = sp.fused && !contiguous ? static_cast<int64_t*>(c.bufs[kSlotOutDst].p)
+                                           : sp.out_src + m;
       fs.last_m = m;
-      fs.last_mask_words = 0;
+      fs.last_mask_words = sp.fused ? 0 : r[3];
       *m_out = m;
       return Status{NLB_OK};
     }

@@ -134,6 +134,13 @@ struct EmitTargets {
   // Pair-task emit only: when set and non-zero (the offsets scan gave up
   // waiting for a tile), nothing is written: the offsets are not valid.
   const int64_t* scan_error;
+  // Pair-task emit only, optional: host-mapped report that block 0 fills as
+  // the launch starts (the list's size is known then): [1] M, [2] the wait
+  // error words (scan_error, grid_scan_error) or-ed, [3] *mask_top, then
+  // [0] = 1.
+  int64_t* report;
+  const int64_t* grid_scan_error;
+  const unsigned long long* mask_top;
   // Batched kernels: 1 = atom indices local to each system (served requests),
   // 0 = global indices (system start added).
   int32_t local_indices;
