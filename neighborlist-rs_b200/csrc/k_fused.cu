@@ -148,9 +148,11 @@ __device__ __forceinline__ uint32_t f_chunk(const GridBuffers& b, const FCell& c
   }
   __syncwarp();
   const float2 ux2 = make_float2(ux, ux), uy2 = make_float2(uy, uy), uz2 = make_float2(uz, uz);
+  const float2 nlo2 = make_float2(-lo, -lo), nhi2 = make_float2(-hi, -hi);
   uint32_t inside = 0, maybe = 0, order = 0;
+  // (candidates 31 down to 0: each predicate's sign bit appended, see push_sign)
 #pragma unroll
-  for (int pr = 0; pr < 16; ++pr) {
+  for (int pr = 15; pr >= 0; --pr) {
     const float4 xy = sxy4[pr];
     const float2 z = sz2[pr];
     const int2 w = sw2[pr];
@@ -158,9 +160,10 @@ __device__ __forceinline__ uint32_t f_chunk(const GridBuffers& b, const FCell& c
     const float2 dy = __fadd2_rn(make_float2(xy.z, xy.w), uy2);
     const float2 dz = __fadd2_rn(z, uz2);
     const float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-    inside |= ((uint32_t)(d2.x < lo) | ((uint32_t)(d2.y < lo) << 1)) << (2 * pr);
-    maybe |= ((uint32_t)(d2.x < hi) | ((uint32_t)(d2.y < hi) << 1)) << (2 * pr);
-    order |= ((uint32_t)(w.x > io_adj) | ((uint32_t)(w.y > io_adj) << 1)) << (2 * pr);
+    const float2 sl = __fadd2_rn(d2, nlo2), sh = __fadd2_rn(d2, nhi2);
+    inside = push_sign(push_sign(inside, __float_as_uint(sl.y)), __float_as_uint(sl.x));
+    maybe = push_sign(push_sign(maybe, __float_as_uint(sh.y)), __float_as_uint(sh.x));
+    order = push_sign(push_sign(order, (uint32_t)(io_adj - w.y)), (uint32_t)(io_adj - w.x));
   }
   __syncwarp();
   if (!live) order = 0;

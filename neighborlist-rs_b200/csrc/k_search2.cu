@@ -499,11 +499,13 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? (K == 1 ? 3 : 1) : (K 
         // with the packed FP32 units (element-wise the same roundings as the
         // scalar dx = x_j + u, d2 = fma(dz, dz, fma(dy, dy, dx * dx))), one
         // squared distance per pair against every cutoff's band.
+        // (candidates 31 down to 0: each predicate's sign bit appended, see
+        // push_sign)
         uint32_t inside[K], maybe[K], order = 0;
 #pragma unroll
         for (int q = 0; q < K; ++q) inside[q] = maybe[q] = 0;
 #pragma unroll
-        for (int pr = 0; pr < 16; ++pr) {
+        for (int pr = 15; pr >= 0; --pr) {
           const float4 xy = stage_xy[warp][pr];
           const float2 z = stage_z[warp][pr];
           const int2 w = stage_w[warp][pr];
@@ -513,10 +515,12 @@ __global__ void __launch_bounds__(kPairWarps * 32, EMIT ? (K == 1 ? 3 : 1) : (K 
           const float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
 #pragma unroll
           for (int q = 0; q < K; ++q) {
-            inside[q] |= ((uint32_t)(d2.x < lo[q]) | ((uint32_t)(d2.y < lo[q]) << 1)) << (2 * pr);
-            maybe[q] |= ((uint32_t)(d2.x < hi[q]) | ((uint32_t)(d2.y < hi[q]) << 1)) << (2 * pr);
+            const float2 sl = __fadd2_rn(d2, make_float2(-lo[q], -lo[q]));
+            const float2 sh = __fadd2_rn(d2, make_float2(-hi[q], -hi[q]));
+            inside[q] = push_sign(push_sign(inside[q], __float_as_uint(sl.y)), __float_as_uint(sl.x));
+            maybe[q] = push_sign(push_sign(maybe[q], __float_as_uint(sh.y)), __float_as_uint(sh.x));
           }
-          order |= ((uint32_t)(w.x > io_adj) | ((uint32_t)(w.y > io_adj) << 1)) << (2 * pr);
+          order = push_sign(push_sign(order, (uint32_t)(io_adj - w.y)), (uint32_t)(io_adj - w.x));
         }
         if (!live) order = 0;
         // Guard bands: the reference's exact FP64 test decides (for every

@@ -65,6 +65,15 @@ __device__ __forceinline__ double norm2(double a, double b, double c) {
 }
 
 // Rust `f as i32`: truncate toward zero, saturate, NaN -> 0.
+// acc << 1 with the sign bit of v as the new lowest bit.  Appending, for
+// candidates 31 down to 0, the sign of (d2 - bound) (FP32, exactly rounded:
+// negative iff d2 < bound for finite or infinite d2) or of (io - j) (no
+// overflow for indices below 2^31 - 1) leaves candidate k's predicate at bit
+// k: one funnel shift per predicate.
+__device__ __forceinline__ uint32_t push_sign(uint32_t acc, uint32_t v) {
+  return __funnelshift_l(v, acc, 1);
+}
+
 __device__ __forceinline__ int32_t sat_i32(double x) {
   if (x != x) return 0;
   if (x >= 2147483647.0) return 2147483647;
