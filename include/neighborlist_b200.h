@@ -62,10 +62,13 @@ int nlb_build_multi(const double* positions, int64_t n_atoms, const double* cuto
                     nlb_result* outs);
 
 /* Batched systems: batch[i] is atom i's system id; a new system starts
- * wherever the id changes (src/batch.rs:25-38).  cells: n_cells x 9 (rows of
- * H as above) or NULL (every system auto-boxed); pbcs: n_cells x 3;
- * has_cell: n_cells flags, 0 = None (auto-box).  Atom indices in the output
- * are global (offset by each system's first atom).
+ * wherever the id changes (src/batch.rs:25-38); ids must not decrease
+ * (NLB_ERR_VALUE "Batch IDs must be monotonic (non-decreasing)", the check of
+ * src/python_api.rs:315-423).  cells: n_cells x 9 (rows of H as above) or
+ * NULL (every system auto-boxed); pbcs: n_cells x 3, or NULL for all
+ * periodic; has_cell: n_cells flags, 0 = None (auto-box), or NULL for all
+ * set.  Atom indices in the output are global (offset by each system's first
+ * atom).
  * Replaces neighborlist_rs::build_neighborlists_batch (src/api.rs:43-84) and
  * batch::search_batch (src/batch.rs:10-147). */
 int nlb_build_batch(const double* positions, int64_t n_atoms, const int32_t* batch,
@@ -373,6 +376,12 @@ void nlb_server_destroy(nlb_server* server);
  * periodic axes only. */
 int nlb_cell_check(const double* cell);
 int nlb_cell_wrap(const double* cell, const uint8_t* pbc, const double* position, double* out);
+/* The batched calls' cell arrays from a (B, 3, 3) stack of ASE cells (rows
+ * = lattice vectors; src/python_api.rs:353-407): h9_out (B x 9) receives
+ * each cell transposed (columns = lattice vectors, the cells argument of
+ * nlb_build_batch), has_out (B) 1 for a cell with a non-zero entry, 0 for an
+ * all-zero one (isolated system, auto-box). */
+void nlb_batch_cells(const double* ase_cells, int64_t n_cells, double* h9_out, uint8_t* has_out);
 
 /* Library version string. */
 const char* nlb_version(void);

@@ -124,35 +124,64 @@ __device__ __forceinline__ void f_describe(const GridParams& g, const GridBuffer
   d.b1 = (int32_t)b.bin_start[r + 1];
 }
 
-// One 32-candidate chunk of a cell for the warp's 32 atoms: the FP32 test of
-// k_search2.cu on packed pairs, the guard band rechecked in FP64, the
-// half-list predicate.  Returns the lane's hit mask.
+// One 32-candidate chunk of a cell for the warp's 32 atoms.  Candidates
+// farther from the group's box (gbox: FP32, in the group's bin frame) than
+// the band allows cannot be within the cutoff of any of its atoms and are
+// dropped first; the kept ones are staged contiguously and go through the
+// FP32 test of k_search2.cu on packed pairs, the guard band rechecked in
+// FP64, the half-list predicate.  Returns the lane's hit mask over the
+// chunk's candidate offsets.
 __device__ __forceinline__ uint32_t f_chunk(const GridBuffers& b, const FCell& cell, int32_t jb,
                                             float ux, float uy, float uz, int32_t io_adj,
                                             bool live, double xi, double yi, double zi, float lo,
-                                            float hi, double rc_sq, float4* sxy4, float2* sz2,
-                                            int2* sw2) {
+                                            float hi, double rc_sq, const float4* gbox,
+                                            float4* sxy4, float2* sz2, int2* sw2,
+                                            uint8_t* smap) {
   const int lane = threadIdx.x & 31;
   const int32_t nj = cell.b1 - jb < 32 ? cell.b1 - jb : 32;
   float4 qv = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(-1));
-  if (lane < nj) qv = b.p32[jb + lane];
+  bool keep = false;
+  if (lane < nj) {
+    qv = b.p32[jb + lane];
+    const float4 glo = gbox[0], ghi = gbox[1];
+    const float cx = qv.x + cell.t[0], cy = qv.y + cell.t[1], cz = qv.z + cell.t[2];
+    const float gx = fmaxf(fmaxf(cx - ghi.x, glo.x - cx), 0.f);
+    const float gy = fmaxf(fmaxf(cy - ghi.y, glo.y - cy), 0.f);
+    const float gz = fmaxf(fmaxf(cz - ghi.z, glo.z - cz), 0.f);
+    // (margin: one band width, as the chunk pruning of k_search2.cu)
+    keep = gx * gx + gy * gy + gz * gz <= hi + (hi - lo);
+  }
+  const uint32_t km = __ballot_sync(0xffffffffu, keep);
+  if (km == 0) return 0;
+  const int nk = __popc(km);
   float* sxy = reinterpret_cast<float*>(sxy4);
   float* sz = reinterpret_cast<float*>(sz2);
   int32_t* sw = reinterpret_cast<int32_t*>(sw2);
-  {
-    const int pr = lane >> 1, h = lane & 1;
+  __syncwarp();  // (the previous chunk's readers are done)
+  if (keep) {
+    const int k = __popc(km & lanemask_lt());
+    const int pr = k >> 1, h = k & 1;
     sxy[4 * pr + h] = qv.x;
     sxy[4 * pr + 2 + h] = qv.y;
     sz[2 * pr + h] = qv.z;
     sw[2 * pr + h] = __float_as_int(qv.w);
+    smap[k] = (uint8_t)lane;
+  }
+  if (lane == 0 && (nk & 1)) {
+    // the odd slot of the last pair: a far sentinel
+    const int pr = nk >> 1;
+    sxy[4 * pr + 1] = 1e30f;
+    sxy[4 * pr + 3] = 1e30f;
+    sz[2 * pr + 1] = 1e30f;
+    sw[2 * pr + 1] = -1;
   }
   __syncwarp();
   const float2 ux2 = make_float2(ux, ux), uy2 = make_float2(uy, uy), uz2 = make_float2(uz, uz);
   const float2 nlo2 = make_float2(-lo, -lo), nhi2 = make_float2(-hi, -hi);
   uint32_t inside = 0, maybe = 0, order = 0;
-  // (candidates 31 down to 0: each predicate's sign bit appended, see push_sign)
-#pragma unroll
-  for (int pr = 15; pr >= 0; --pr) {
+  // (kept candidates from the last down to 0: each predicate's sign bit
+  // appended, see push_sign, leaves kept candidate k at bit k)
+  for (int pr = ((nk + 1) >> 1) - 1; pr >= 0; --pr) {
     const float4 xy = sxy4[pr];
     const float2 z = sz2[pr];
     const int2 w = sw2[pr];
@@ -165,19 +194,27 @@ __device__ __forceinline__ uint32_t f_chunk(const GridBuffers& b, const FCell& c
     maybe = push_sign(push_sign(maybe, __float_as_uint(sh.y)), __float_as_uint(sh.x));
     order = push_sign(push_sign(order, (uint32_t)(io_adj - w.y)), (uint32_t)(io_adj - w.x));
   }
-  __syncwarp();
   if (!live) order = 0;
   uint32_t amb = maybe & ~inside & order;
   while (amb) {
-    const int jj = __ffs(amb) - 1;
+    const int k = __ffs(amb) - 1;
     amb &= amb - 1;
-    const int32_t j = jb + jj;
+    const int32_t j = jb + smap[k];
     const double ex = dadd(dsub(b.px[j], xi), cell.off[0]);
     const double ey = dadd(dsub(b.py[j], yi), cell.off[1]);
     const double ez = dadd(dsub(b.pz[j], zi), cell.off[2]);
-    if (norm2(ex, ey, ez) < rc_sq) inside |= 1u << jj;
+    if (norm2(ex, ey, ez) < rc_sq) inside |= 1u << k;
   }
-  return inside & order;
+  uint32_t hk = inside & order;
+  // Kept candidate k back to its offset in the chunk.
+  if (km == (nj == 32 ? 0xffffffffu : (1u << nj) - 1u)) return hk;
+  uint32_t hits = 0;
+  while (hk) {
+    const int k = __ffs(hk) - 1;
+    hk &= hk - 1;
+    hits |= 1u << smap[k];
+  }
+  return hits;
 }
 
 // Irregular atom p (its home stencil is not its stored bin): one warp walks
@@ -250,6 +287,8 @@ __global__ void __launch_bounds__(kFThreads, 4)
   __shared__ float4 st_xy[kFWarps][16];
   __shared__ float2 st_z[kFWarps][16];
   __shared__ int2 st_w[kFWarps][16];
+  __shared__ uint8_t st_map[kFWarps][32];
+  __shared__ float4 s_gbox[2];  // the group's FP32 box in its bin frame
   __shared__ SlotMeta lmeta[32];
   __shared__ int64_t abase[33];
   __shared__ int32_t s_ticket, s_irr, s_big, s_skip, s_cell;
@@ -290,6 +329,25 @@ __global__ void __launch_bounds__(kFThreads, 4)
       cells[c] = d;
     }
     if (warp == 1 && lane < len) lmeta[lane] = b.meta[p];
+    if (warp == 2) {
+      // The group's box (its atoms' packed FP32 positions; lanes past len
+      // repeat the first atom).
+      const float4 q = b.p32[p];
+      float4 lo4 = q, hi4 = q;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lo4.x = fminf(lo4.x, __shfl_xor_sync(0xffffffffu, lo4.x, o));
+        lo4.y = fminf(lo4.y, __shfl_xor_sync(0xffffffffu, lo4.y, o));
+        lo4.z = fminf(lo4.z, __shfl_xor_sync(0xffffffffu, lo4.z, o));
+        hi4.x = fmaxf(hi4.x, __shfl_xor_sync(0xffffffffu, hi4.x, o));
+        hi4.y = fmaxf(hi4.y, __shfl_xor_sync(0xffffffffu, hi4.y, o));
+        hi4.z = fmaxf(hi4.z, __shfl_xor_sync(0xffffffffu, hi4.z, o));
+      }
+      if (lane == 0) {
+        s_gbox[0] = lo4;
+        s_gbox[1] = hi4;
+      }
+    }
     __syncthreads();
     if (tid == 0) {
       // Masks stay in shared memory while they fit, cell by cell.
@@ -329,7 +387,8 @@ __global__ void __launch_bounds__(kFThreads, 4)
         const float ux = cell.t[0] - a.x, uy = cell.t[1] - a.y, uz = cell.t[2] - a.z;
         for (int32_t jb = cell.b0; jb < cell.b1; jb += 32) {
           const uint32_t hits = f_chunk(b, cell, jb, ux, uy, uz, io_adj, live, xi, yi, zi, lo, hi,
-                                        rc_sq, st_xy[warp], st_z[warp], st_w[warp]);
+                                        rc_sq, s_gbox, st_xy[warp], st_z[warp], st_w[warp],
+                                        st_map[warp]);
           cnt += __popc(hits);
           if (cell.mbase >= 0) masks[cell.mbase + (jb - cell.b0) + lane] = hits;
         }
@@ -397,7 +456,7 @@ __global__ void __launch_bounds__(kFThreads, 4)
             hits = masks[cell.mbase + (jb - cell.b0) + lane];
           else
             hits = f_chunk(b, cell, jb, ux, uy, uz, io_adj, live, xi, yi, zi, lo, hi, rc_sq,
-                           st_xy[warp], st_z[warp], st_w[warp]);
+                           s_gbox, st_xy[warp], st_z[warp], st_w[warp], st_map[warp]);
           if (!need) hits = 0;
           while (hits) {
             const int jj = __ffs(hits) - 1;
@@ -510,7 +569,7 @@ __global__ void __launch_bounds__(kFThreads, 4)
             hits = masks[cell.mbase + (jb - cell.b0) + lane];
           else
             hits = f_chunk(b, cell, jb, ux, uy, uz, io_adj, live, xi, yi, zi, lo, hi, rc_sq,
-                           st_xy[warp], st_z[warp], st_w[warp]);
+                           s_gbox, st_xy[warp], st_z[warp], st_w[warp], st_map[warp]);
           if (!need) hits = 0;
           while (hits) {
             const int jj = __ffs(hits) - 1;

@@ -1350,6 +1350,20 @@ int nlb_cell_check(const double* cell) {
   return NLB_OK;
 }
 
+void nlb_batch_cells(const double* ase_cells, int64_t n_cells, double* h9_out, uint8_t* has_out) {
+  for (int64_t i = 0; i < n_cells; ++i) {
+    const double* r = ase_cells + 9 * i;
+    double* h = h9_out + 9 * i;
+    bool any = false;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        h[3 * a + b] = r[3 * b + a];
+        any = any || r[3 * b + a] != 0.0;
+      }
+    has_out[i] = any ? 1 : 0;
+  }
+}
+
 int nlb_cell_wrap(const double* cell, const uint8_t* pbc, const double* p, double* out) {
   if (!cell || !p || !out) return fail(NLB_ERR_VALUE, "NULL argument").code;
   HostCell c;

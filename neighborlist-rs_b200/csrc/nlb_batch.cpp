@@ -575,8 +575,12 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
 
   std::vector<int64_t> starts;
   starts.push_back(0);
-  for (int64_t i = 1; i < n; ++i)
-    if (batch[i] != batch[i - 1]) starts.push_back(i);
+  for (int64_t i = 1; i < n; ++i) {
+    if (batch[i] == batch[i - 1]) continue;
+    if (batch[i] < batch[i - 1])
+      return fail(NLB_ERR_VALUE, "Batch IDs must be monotonic (non-decreasing)");
+    starts.push_back(i);
+  }
   starts.push_back(n);
   const int32_t n_sys = (int32_t)starts.size() - 1;
   const int64_t have = cells ? n_cells : (int64_t)n_sys;

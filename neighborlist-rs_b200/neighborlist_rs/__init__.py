@@ -286,16 +286,20 @@ def build_multi_from_ase(atoms, cutoffs, labels=None, disjoint=False):
 
 
 def _batch_cells(cells, batch, need_count=False):
-    """Monotonic check and the (B,3,3) cells -> C arrays (src/python_api.rs:
-    353-407): a zero matrix means isolated (auto-box); any other cell is
-    transposed from ASE rows and gets pbc (T, T, T).  Every given cell is
-    passed on; the library splits the systems and reports "Expected at least
-    {n} cells, but got {m}" when there are fewer cells than systems.  The
-    system count is computed here only when the caller needs it."""
-    b1, b0 = batch[1:], batch[:-1]
-    if (b1 < b0).any():
-        raise ValueError("Batch IDs must be monotonic (non-decreasing)")
-    n_sys = 1 + int(np.count_nonzero(b1 != b0)) if need_count else -1
+    """The (B,3,3) cells -> C arrays (src/python_api.rs:353-407): a zero
+    matrix means isolated (auto-box); any other cell is transposed from ASE
+    rows and gets pbc (T, T, T) (pbcs None: the library's default).  Every
+    given cell is passed on; the library splits the systems and reports
+    "Batch IDs must be monotonic (non-decreasing)" and "Expected at least {n}
+    cells, but got {m}".  The system count is computed here only when the
+    caller needs it (it is then also where a non-monotonic batch is
+    reported)."""
+    n_sys = -1
+    if need_count:
+        b1, b0 = batch[1:], batch[:-1]
+        if (b1 < b0).any():
+            raise ValueError("Batch IDs must be monotonic (non-decreasing)")
+        n_sys = 1 + int(np.count_nonzero(b1 != b0))
     if cells is None:
         return n_sys, None, None, None, 0
     if not isinstance(cells, np.ndarray) or cells.ndim != 3 or cells.dtype != np.float64:
@@ -303,10 +307,15 @@ def _batch_cells(cells, batch, need_count=False):
     if cells.shape[1:] != (3, 3):
         raise ValueError("cells must have shape (B, 3, 3)")
     nc = cells.shape[0]
-    has = np.any(cells != 0.0, axis=(1, 2)).astype(np.uint8)
-    h9 = np.ascontiguousarray(np.transpose(cells, (0, 2, 1)).reshape(nc, 9))
-    pbcs = np.ones((nc, 3), np.uint8)
-    return n_sys, h9, pbcs, has, nc
+    h9 = np.empty((nc, 9), np.float64)
+    has = np.empty(nc, np.uint8)
+    _lib.nlb_batch_cells(np.ascontiguousarray(cells).ctypes.data_as(_dp), nc,
+                         h9.ctypes.data_as(_dp), has.ctypes.data_as(_u8p))
+    return n_sys, h9, None, has, nc
+
+
+_lib.nlb_batch_cells.argtypes = [_dp, ctypes.c_int64, _dp, _u8p]
+_lib.nlb_batch_cells.restype = None
 
 
 def build_neighborlists_batch(positions, batch, cells=None, cutoff=5.0, parallel=True, *,
