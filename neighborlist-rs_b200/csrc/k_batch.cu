@@ -659,6 +659,21 @@ __global__ void k_sys_bounds(const SysPlan* __restrict__ plans, int n_sys,
   if (s == n_sys) out[s] = offs[row - 1] - offs[0];
 }
 
+// Position of the k-th (from 0) set bit of m (k < popc(m)).
+__device__ __forceinline__ int select_bit(uint32_t m, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w >= 1; w >>= 1) {
+    const int c = __popc(m & ((1u << w) - 1u));
+    if (k >= c) {
+      k -= c;
+      m >>= w;
+      pos += w;
+    }
+  }
+  return pos;
+}
+
 // Expansion of the count pass's records into the single-cutoff list: one
 // warp per segment; each record's hit lanes write (i, j, shift) at the
 // atom's next slots, in record order -- the order the recomputing emit pass
@@ -693,7 +708,7 @@ __global__ void __launch_bounds__(256)
       my_j = r[1];
       my_sh = r[2];
     }
-    int64_t cur = t.base[0] + (offs[hdr.x] - offs[0]) + hdr.y;
+    const int64_t cur = t.base[0] + (offs[hdr.x] - offs[0]) + hdr.y;
     const int64_t idx_off = t.local_indices ? t.index_offset : start + t.index_offset;
     int64_t* src = t.src[0];
     int64_t* dst = t.dst[0];
@@ -711,12 +726,36 @@ __global__ void __launch_bounds__(256)
       yi = pi[1];
       zi = pi[2];
     }
-    for (int r = 0; r < hdr.z; ++r) {
+    // The segment's hits are consecutive in the list: hit h (records in
+    // order, bits in order) goes to slot cur + h.  Each lane takes hits h =
+    // lane, lane + 32, ...: its record by a binary search over the records'
+    // inclusive hit counts, its candidate as that record's (h - first)-th
+    // set bit; the warp's stores are contiguous.
+    const int c = __popc(my_mask);
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - c;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+#pragma unroll 2
+    for (int h0 = 0; h0 < total; h0 += 32) {
+      const int h = h0 + lane;
+      int r = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int v = __shfl_sync(0xffffffffu, incl, r + step - 1);
+        if (v <= h) r += step;
+      }
       const uint32_t mask = __shfl_sync(0xffffffffu, my_mask, r);
       const int32_t j0 = (int32_t)__shfl_sync(0xffffffffu, my_j, r);
       const uint32_t psh = __shfl_sync(0xffffffffu, my_sh, r);
-      if ((mask >> lane) & 1u) {
-        const SlotMeta mj = rb.meta[slot + j0 + lane];
+      const int first = __shfl_sync(0xffffffffu, excl, r);
+      if (h < total) {
+        const int jj = select_bit(mask, h - first);
+        const SlotMeta mj = rb.meta[slot + j0 + jj];
         int32_t s[3];
         if (method == 1) {
           const double* pj = pos + 3 * (start + mj.orig);
@@ -729,7 +768,7 @@ __global__ void __launch_bounds__(256)
           s[1] = (mj.sy - mi.sy) + ((int32_t)(psh << 12) >> 22);
           s[2] = (mj.sz - mi.sz) + ((int32_t)(psh << 2) >> 22);
         }
-        const int64_t e = cur + __popc(mask & lanemask_lt());
+        const int64_t e = cur + h;
         src[e] = (int64_t)mi.orig + idx_off;
         dst[e] = (int64_t)mj.orig + idx_off;
         int32_t* sp = t.sh[0] + 3 * e;
@@ -737,7 +776,6 @@ __global__ void __launch_bounds__(256)
         sp[1] = s[1];
         sp[2] = s[2];
       }
-      cur += __popc(mask);
     }
   }
 }
