@@ -681,7 +681,7 @@ __device__ __forceinline__ int select_bit(uint32_t m, int k) {
 // wrap shifts and image for raw brute force); the minimum-image systems
 // recompute the pair's shift from the raw positions exactly as the count
 // pass did.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_batch_expand(BatchRecords rb, const SysPlan* __restrict__ plans,
                    const double* __restrict__ pos, const int64_t* __restrict__ offs, int64_t row,
                    EmitTargets t) {
@@ -694,20 +694,38 @@ __global__ void __launch_bounds__(256)
   const int n_seg = min(*rb.seg_top, rb.seg_cap);
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int sg = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); sg < n_seg; sg += warps) {
-    const int4 hdr = rb.seg_hdr[sg];
+  // (the next segment's header and records are loaded while this one is
+  // written)
+  int sg = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int4 hdr_next = make_int4(0, 0, 0, 0);
+  uint32_t rec_next[3] = {0u, 0u, 0u};
+  if (sg < n_seg) {
+    hdr_next = rb.seg_hdr[sg];
+    const uint32_t* r = rb.rec + ((size_t)sg * 32 + lane) * 3;
+    rec_next[0] = r[0];
+    rec_next[1] = r[1];
+    rec_next[2] = r[2];
+  }
+  for (; sg < n_seg; sg += warps) {
+    const int4 hdr = hdr_next;
+    uint32_t my_mask = 0, my_j = 0, my_sh = 0;
+    if (lane < hdr.z) {
+      my_mask = rec_next[0];
+      my_j = rec_next[1];
+      my_sh = rec_next[2];
+    }
+    if (sg + warps < n_seg) {
+      hdr_next = rb.seg_hdr[sg + warps];
+      const uint32_t* r = rb.rec + ((size_t)(sg + warps) * 32 + lane) * 3;
+      rec_next[0] = r[0];
+      rec_next[1] = r[1];
+      rec_next[2] = r[2];
+    }
     const SysPlan* P = plans + hdr.w;
     const int32_t method = P->method;
     const int64_t start = P->start;
     const int32_t slot = P->slot;
     const SlotMeta mi = rb.meta[hdr.x];
-    uint32_t my_mask = 0, my_j = 0, my_sh = 0;
-    if (lane < hdr.z) {
-      const uint32_t* r = rb.rec + ((size_t)sg * 32 + lane) * 3;
-      my_mask = r[0];
-      my_j = r[1];
-      my_sh = r[2];
-    }
     const int64_t cur = t.base[0] + (offs[hdr.x] - offs[0]) + hdr.y;
     const int64_t idx_off = t.local_indices ? t.index_offset : start + t.index_offset;
     int64_t* src = t.src[0];
