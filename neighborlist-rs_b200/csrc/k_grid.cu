@@ -25,6 +25,7 @@ namespace {
 constexpr int kSortThreads = 128;
 constexpr int kSortCap = 2048;  // elements sorted entirely in shared memory
 constexpr int64_t kRankSortMax = 512;  // bins up to this size: rank placement
+constexpr int kPlaceSplit = 4;         // threads per atom in the rank placement
 
 // Grid points p (0 <= p_a < nb_a) whose Morton code is smaller than that of c.
 __device__ int64_t morton_rank(const int32_t c[3], const int32_t nb[3]) {
@@ -402,9 +403,9 @@ __device__ void sort_bin(const GridParams& g, const double* __restrict__ pos, in
   if (p32 && threadIdx.x == 0) store_groups(g, r, s, e, lin0, groups, counters, group_start);
 }
 
-// Places every atom at its slot.  Blocks [0, atom_blocks): one thread per
-// entry p of the bin segments k_scatter wrote (arbitrary order inside a
-// segment); for bins of at most kRankSortMax atoms the atom's place in its
+// Places every atom at its slot.  Blocks [0, atom_blocks): kPlaceSplit
+// threads per entry p of the bin segments k_scatter wrote (arbitrary order
+// inside a segment); for bins of at most kRankSortMax atoms the atom's place in its
 // bin is the number of the bin's (key, index) pairs below its own (a rank
 // sort: the bin's pairs are read by each of its atoms, from L1), and the
 // thread writes the slot there directly; the atom placed first writes the
@@ -431,15 +432,23 @@ __global__ void __launch_bounds__(kSortThreads)
              irr_list, irr, counters, cbox, group_start, sk, sv);
     return;
   }
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
+  // (kPlaceSplit consecutive threads per entry, each counting a strided
+  // share of the bin: more loads in flight than one thread per atom)
+  const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kPlaceSplit;
+  const int part = (int)(threadIdx.x % kPlaceSplit);
+  if (p >= n) return;  // (the same for the entry's threads, as below)
   const uint64_t k = skey[p];
   const int32_t i = sidx[p];
   const int32_t r = rank[i];
   const int64_t s = bin_start[r], e = bin_start[r + 1];
   if (e - s > kRankSortMax) return;
   int32_t below = 0;
-  for (int64_t q = s; q < e; ++q) below += pair_less(__ldg(&skey[q]), __ldg(&sidx[q]), k, i) ? 1 : 0;
+  for (int64_t q = s + part; q < e; q += kPlaceSplit)
+    below += pair_less(__ldg(&skey[q]), __ldg(&sidx[q]), k, i) ? 1 : 0;
+  const unsigned group = ((1u << kPlaceSplit) - 1u) << (threadIdx.x & 31 & ~(kPlaceSplit - 1));
+#pragma unroll
+  for (int o = 1; o < kPlaceSplit; o <<= 1) below += __shfl_xor_sync(group, below, o);
+  if (part != 0) return;
   const SlotOut so = store_slot(g, pos, s + below, i, px, py, pz, meta, p32, sbin, irr_list, irr,
                                 counters);
   if (p32 && below == 0) store_groups(g, r, s, e, so.lin, groups, counters, group_start);
@@ -524,7 +533,7 @@ void launch_grid_build(const GridParams& g, const double* pos, int64_t n, const 
   if (!fused) exclusive_scan_i32(b.bin_count, g.total_bins, b.bin_start, b.scan_tmp, s);
   launch_pdl(k_scatter, dim3((unsigned)((n + T - 1) / T)), dim3(T), 0, s, b.key, b.rank, n,
              b.bin_start, b.bin_fill, b.skey, b.sidx, (const int32_t*)b.fill);
-  const int32_t atom_blocks = (int32_t)((n + kSortThreads - 1) / kSortThreads);
+  const int32_t atom_blocks = (int32_t)((kPlaceSplit * n + kSortThreads - 1) / kSortThreads);
   launch_pdl(k_place, dim3((unsigned)(atom_blocks + g.total_bins)), dim3(kSortThreads), 0, s, g,
              pos, n, (const int32_t*)b.rank, (const int64_t*)b.bin_start, b.skey, b.sidx, b.skey2,
              b.sidx2, b.px, b.py, b.pz, b.meta, b.p32, b.sbin, b.groups, b.irr_list, b.irr,
