@@ -25,8 +25,9 @@
 //      memory and storing them with consecutive threads on consecutive slots.
 //
 // Sources and shifts go to their arrays at slot e, destinations to a
-// separate array (the total M is known only when the last group is done; the
-// host moves the destinations behind the sources when it needs [src | dst]).
+// separate array (the total M is known only when the last group is done);
+// for [src | dst] the CTAs then move the destinations behind the sources
+// once every group is written.
 // The last group writes M.  A group whose block does not fit the capacity
 // writes nothing (the host grows the arrays and runs the launch again).
 // Atoms whose home stencil differs from their stored bin ("irregular",
@@ -609,6 +610,28 @@ __global__ void __launch_bounds__(kFThreads, 4)
     *o.total = 0;
     f_report(o, 0, 0);
   }
+  if (!o.move || n_groups == 0) return;
+  // [src | dst]: once every group is written (all tickets are taken by
+  // running CTAs, so the wait ends; bounded all the same), each CTA moves
+  // its stride of the destinations behind the M sources.
+  if (tid == 0) {
+    int spins = 0;
+    unsigned long long d = *reinterpret_cast<volatile unsigned long long*>(o.done);
+    while (d < (unsigned long long)n_groups && spins < o.spin_limit) {
+      __nanosleep(64);
+      d = *reinterpret_cast<volatile unsigned long long*>(o.done);
+      ++spins;
+    }
+    s_skip = d >= (unsigned long long)n_groups ? 0 : 1;
+    if (s_skip) atomicExch(reinterpret_cast<unsigned long long*>(&o.state[1]), 1ull);
+  }
+  __syncthreads();
+  if (s_skip) return;
+  __threadfence();
+  const int64_t m = *reinterpret_cast<volatile int64_t*>(o.total);
+  if (m > o.capacity) return;
+  for (int64_t e = (int64_t)blockIdx.x * kFThreads + tid; e < m; e += (int64_t)gridDim.x * kFThreads)
+    o.src[m + e] = __ldcg(&o.dst[e]);
 }
 
 }  // namespace
@@ -616,29 +639,6 @@ __global__ void __launch_bounds__(kFThreads, 4)
 size_t fused_smem_bytes(int32_t n_cells, int32_t mask_words) {
   return fused_cells_bytes(n_cells) + sizeof(uint32_t) * (((size_t)n_cells + 1) * 32 + mask_words +
                                                            kFStage);
-}
-
-namespace {
-
-__global__ void k_move_dst(int64_t* __restrict__ src, const int64_t* __restrict__ dst,
-                           const int64_t* __restrict__ total, int64_t capacity) {
-  pdl_wait();
-  const int64_t m = *total;
-  if (m > capacity) return;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m;
-       e += (int64_t)gridDim.x * blockDim.x)
-    src[m + e] = dst[e];
-}
-
-}  // namespace
-
-void launch_move_dst(int64_t* src, const int64_t* dst, const int64_t* total, int64_t capacity,
-                     cudaStream_t s) {
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  launch_pdl(k_move_dst, dim3((unsigned)(sms * 4)), dim3(256), 0, s, src, dst, total, capacity);
-  note_launches(1);
 }
 
 void launch_pair_fused(const GridParams& g, const GridBuffers& b, int32_t n_cells,

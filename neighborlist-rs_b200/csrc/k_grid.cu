@@ -25,7 +25,7 @@ namespace {
 constexpr int kSortThreads = 128;
 constexpr int kSortCap = 2048;  // elements sorted entirely in shared memory
 constexpr int64_t kRankSortMax = 512;  // bins up to this size: rank placement
-constexpr int kPlaceSplit = 4;         // threads per atom in the rank placement
+constexpr int kPlaceSplit = 8;         // threads per atom in the rank placement
 
 // Grid points p (0 <= p_a < nb_a) whose Morton code is smaller than that of c.
 __device__ int64_t morton_rank(const int32_t c[3], const int32_t nb[3]) {

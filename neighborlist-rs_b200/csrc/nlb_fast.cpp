@@ -206,9 +206,9 @@ FusedOut fused_targets(Ctx& c, const SystemPlan& sp, int64_t capacity) {
 
 // The fused launch (and the move of the destinations behind the sources).
 void issue_fused(Ctx& c, SystemPlan& sp, int64_t capacity, bool contiguous) {
-  const FusedOut o = fused_targets(c, sp, capacity);
+  FusedOut o = fused_targets(c, sp, capacity);
+  o.move = contiguous ? 1 : 0;
   launch_pair_fused(sp.grid, sp.gb, (int32_t)stencil_cells_of(sp.grid), sp.band, o, c.stream);
-  if (contiguous) launch_move_dst(o.src, o.dst, o.total, capacity, c.stream);
 }
 
 EmitTargets fast_targets(const SystemPlan& sp, int64_t capacity, int64_t* report = nullptr) {

@@ -204,6 +204,9 @@ struct FusedOut {
   // for the launch (or the ones queued after it) to end.
   unsigned long long* done;
   int64_t* report;
+  // 1: after the last group, the CTAs move the M destinations behind the M
+  // sources (src[M + e] = dst[e]: the [src | dst] layout of device results).
+  int32_t move;
   int32_t spin_limit; // polls of one look-back wait before it gives up
   int32_t withhold;   // failure-detection hook: this group never publishes (-1: none)
   int32_t mask_words; // hit-mask words per group in shared memory
@@ -212,10 +215,6 @@ __host__ __device__ inline size_t fused_cells_bytes(int32_t n_cells) {
   return ((size_t)88 * (size_t)n_cells + 15) & ~(size_t)15;
 }
 size_t fused_smem_bytes(int32_t n_cells, int32_t mask_words);
-// Moves the M destinations of the fused kernel behind the M sources (reads
-// M from *total; nothing when M > capacity).
-void launch_move_dst(int64_t* src, const int64_t* dst, const int64_t* total, int64_t capacity,
-                     cudaStream_t s);
 constexpr int32_t kFusedSpinLimit = 1 << 22;
 void launch_pair_fused(const GridParams& g, const GridBuffers& b, int32_t n_cells,
                        const GuardBand& band, const FusedOut& o, cudaStream_t s);
