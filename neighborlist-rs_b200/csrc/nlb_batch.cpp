@@ -8,6 +8,10 @@
 // are concatenated in system order with atom indices offset by each system's
 // first atom, and each system is planned exactly like a single call (auto-box
 // margin and mic_safe from the largest cutoff).
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -557,6 +561,33 @@ void release_batch_graphs() {
   }
 }
 
+// First atom of every system (a new system wherever the id changes) and n
+// at the end; false when an id decreases.  Four ids per step with SSE2:
+// most steps hold no change.
+bool batch_starts(const int32_t* batch, int64_t n, std::vector<int64_t>& starts) {
+  starts.clear();
+  starts.push_back(0);
+  int64_t i = 1;
+#if defined(__SSE2__)
+  for (; i + 4 <= n; i += 4) {
+    const __m128i cur = _mm_loadu_si128(reinterpret_cast<const __m128i*>(batch + i));
+    const __m128i prv = _mm_loadu_si128(reinterpret_cast<const __m128i*>(batch + i - 1));
+    const int changed = _mm_movemask_ps(_mm_castsi128_ps(_mm_cmpeq_epi32(cur, prv))) ^ 0xF;
+    if (!changed) continue;
+    if (_mm_movemask_ps(_mm_castsi128_ps(_mm_cmpgt_epi32(prv, cur))) != 0) return false;
+    for (int k = 0; k < 4; ++k)
+      if ((changed >> k) & 1) starts.push_back(i + k);
+  }
+#endif
+  for (; i < n; ++i) {
+    if (batch[i] == batch[i - 1]) continue;
+    if (batch[i] < batch[i - 1]) return false;
+    starts.push_back(i);
+  }
+  starts.push_back(n);
+  return true;
+}
+
 Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_batch,
                  const double* cutoffs, int32_t k, const double* cells, const uint8_t* pbcs,
                  const uint8_t* has_cell, int64_t n_cells, bool disjoint, bool multi,
@@ -574,14 +605,8 @@ Status run_batch(const double* pos, int64_t n, const int32_t* batch, int64_t n_b
   if (!pos || !batch) return fail(NLB_ERR_VALUE, "positions or batch is NULL");
 
   std::vector<int64_t> starts;
-  starts.push_back(0);
-  for (int64_t i = 1; i < n; ++i) {
-    if (batch[i] == batch[i - 1]) continue;
-    if (batch[i] < batch[i - 1])
-      return fail(NLB_ERR_VALUE, "Batch IDs must be monotonic (non-decreasing)");
-    starts.push_back(i);
-  }
-  starts.push_back(n);
+  if (!batch_starts(batch, n, starts))
+    return fail(NLB_ERR_VALUE, "Batch IDs must be monotonic (non-decreasing)");
   const int32_t n_sys = (int32_t)starts.size() - 1;
   const int64_t have = cells ? n_cells : (int64_t)n_sys;
   if (have < (int64_t)n_sys)
