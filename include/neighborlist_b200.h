@@ -126,7 +126,13 @@ void nlb_set_stack_threshold(size_t v);
  * valid until that thread's next build call (copy them out to keep them).
  * Layout is the same as nlb_result (edge_index = [src | dst], shift xyz).
  * Used by GNN pipelines that consume edge_index on the GPU (e.g. through
- * DLPack / torch) and by bench.py's device-resident measurement. */
+ * DLPack / torch) and by bench.py's device-resident measurement.
+ * Ordering: on the library's own stream the call returns when the arrays are
+ * complete.  On a stream set with nlb_set_stream it returns as soon as M is
+ * known (the device reports it through host-mapped memory); the arrays are
+ * complete in that stream's order -- work queued on it afterwards sees them,
+ * work on other streams must wait for it (an event).  The same holds for
+ * nlb_build_device_owned. */
 typedef struct nlb_device_result {
   int64_t n_edges;
   int64_t* edge_index; /* device, 2*M int64 */
