@@ -10,9 +10,9 @@
 //   k_scatter    : atoms -> bin segments (arbitrary order inside a segment).
 //   k_place      : every atom to its slot (wrapped positions, wrap shifts,
 //                  original indices, packed FP32 positions, group records):
-//                  in bins of at most kRankSortMax atoms one thread per atom
-//                  counts the bin's (key, index) pairs below its own (rank
-//                  sort); larger bins are sorted by one CTA each -- bitonic in
+//                  in bins of at most kRankSortMax atoms kPlaceSplit threads
+//                  per atom count the bin's (key, index) pairs below its own
+//                  (rank sort); larger bins are sorted by one CTA each -- bitonic in
 //                  shared memory up to kSortCap, merge path through global
 //                  scratch above it.
 //   k_chunk_box  : bounding box of each 32-atom chunk (dense grids only).

@@ -108,3 +108,50 @@ def test_torch_results_zero_copy_and_oracle(nl, oracle):
         want = oracle.search_single(p, None if rows_t is None else rows_t.T,
                                     None if rows_t is None else PBC3, rc)
         assert_same(as_np(got), want, f"small system rc {rc}")
+
+
+def test_builds_on_two_streams_without_host_sync(nl, oracle):
+    """A build on a caller's stream returns as soon as M is known; the next
+    build on another stream reuses the workspace only after that work (the
+    library orders it on the device).  Both lists, read after the fact, equal
+    the oracle's; so do raw workspace results read on the producing stream
+    right after the call."""
+    import torch
+
+    from neighborlist_rs import workloads as W
+
+    pos_a, rows_a = W.cluster_liquid(n_clusters=1112, box=46.4, seed=3)
+    pos_b, rows_b = W.cluster_liquid(n_clusters=600, box=38.0, seed=9)
+    cell_a, cell_b = nl.PyCell(rows_a.T.tolist()), nl.PyCell(rows_b.T.tolist())
+    sa, sb = torch.cuda.Stream(), torch.cuda.Stream()
+    with torch.cuda.stream(sa):
+        da = torch.from_numpy(pos_a).cuda()
+    with torch.cuda.stream(sb):
+        db = torch.from_numpy(pos_b).cuda()
+    torch.cuda.synchronize()
+    for _ in range(3):
+        with torch.cuda.stream(sa):
+            ra = nl.build_neighborlists_torch(cell_a, da, 6.0)
+        with torch.cuda.stream(sb):
+            rb = nl.build_neighborlists_torch(cell_b, db, 6.0)
+        torch.cuda.synchronize()
+        assert_same(as_np(ra), oracle.search_single(pos_a, rows_a.T, PBC3, 6.0, nthreads=8),
+                    "stream A")
+        assert_same(as_np(rb), oracle.search_single(pos_b, rows_b.T, PBC3, 6.0, nthreads=8),
+                    "stream B")
+    # Raw workspace results, copied out on the producing stream at once.
+    nl.set_stream(sa.cuda_stream)
+    try:
+        m, ei_ptr, sh_ptr = nl.build_device_raw(cell_a, da.data_ptr(), pos_a.shape[0], 6.0)
+        with torch.cuda.stream(sa):
+            ei = torch.empty((2, m), dtype=torch.int64, device="cuda")
+            sh = torch.empty((m, 3), dtype=torch.int32, device="cuda")
+            assert nl._lib.nlb_copy_device(ctypes.c_void_p(ei.data_ptr()), ctypes.c_void_p(ei_ptr),
+                                           16 * m, ctypes.c_void_p(sa.cuda_stream)) == 0
+            assert nl._lib.nlb_copy_device(ctypes.c_void_p(sh.data_ptr()), ctypes.c_void_p(sh_ptr),
+                                           12 * m, ctypes.c_void_p(sa.cuda_stream)) == 0
+    finally:
+        nl.set_stream(None)
+    torch.cuda.synchronize()
+    assert_same(as_np({"edge_index": ei, "shift": sh}),
+                oracle.search_single(pos_a, rows_a.T, PBC3, 6.0, nthreads=8), "raw on stream A")
