@@ -878,7 +878,9 @@ Status run_single(const double* pos, int64_t n, const double* cell9, const uint8
   if (!st.ok()) return st;
   if (fast_eligible(sp)) {
     int64_t m = 0;
-    st = run_fast(*c, sp, d_pos, &m, false);  // (host copies: no [src | dst] layout needed)
+    // (host copies: no [src | dst] layout needed; the copies follow the
+    // search on the stream, so the call goes on as soon as M is known)
+    st = run_fast(*c, sp, d_pos, &m, false, true);
     if (!st.ok()) return st;
     DevLists L;
     L.src.assign(1, sp.out_src);

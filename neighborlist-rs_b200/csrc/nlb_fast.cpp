@@ -280,7 +280,8 @@ Status wait_report(Ctx& c) {
 // returns at once: the remaining work (the emit, or the move of the
 // destinations) is queued on that stream ahead of anything the caller queues
 // there.  On the library's own stream it also waits for that work.
-Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, bool contiguous) {
+Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, bool contiguous,
+                bool stream_ordered) {
   FastState& fs = state_for(c);
   const int64_t n_cells = stencil_cells_of(sp.grid);
   sp.fused = single_pipeline_mode() == 0 && n_cells <= kFusedMaxCells &&
@@ -376,8 +377,10 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, boo
     if (r[2] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
     if (m <= capacity) {
       if (c.stream == c.own_stream) {
-        const cudaError_t e = cudaStreamSynchronize(c.stream);
-        if (e != cudaSuccess) return cuda_fail(e, "neighbour-list pipeline");
+        if (!stream_ordered) {
+          const cudaError_t e = cudaStreamSynchronize(c.stream);
+          if (e != cudaSuccess) return cuda_fail(e, "neighbour-list pipeline");
+        }
       } else {
         const cudaError_t e = cudaEventRecord(c.early_ev, c.stream);
         if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");

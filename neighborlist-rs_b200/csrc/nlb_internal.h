@@ -207,8 +207,11 @@ Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& 
 // (sources), sp.out_dst (destinations) and sp.out_sh.  contiguous = true
 // puts the destinations right behind the sources (sp.out_dst = out_src + M,
 // the [src | dst] layout); otherwise they may stay in a separate array.
+// stream_ordered = true: the caller only queues further work on c.stream
+// (e.g. the result copies) and synchronises it itself, so the call returns
+// as soon as M is known even on the library's own stream.
 Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out,
-                bool contiguous = true);
+                bool contiguous = true, bool stream_ordered = false);
 // Single-system pipeline choice: 0 = automatic (the one-launch kernel on
 // sparse grids), 1 = always the three-launch pair-task pipeline.
 int32_t single_pipeline_mode();
