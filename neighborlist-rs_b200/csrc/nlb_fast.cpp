@@ -265,7 +265,12 @@ Status wait_report(Ctx& c) {
     const cudaError_t q = cudaStreamQuery(c.stream);
     if (q == cudaErrorNotReady) continue;
     if (q != cudaSuccess) return cuda_fail(q, "neighbour-list pipeline");
-    if (r[0] == 0) return fail(NLB_ERR_CUDA, "the search ended without its report");
+    if (r[0] == 0) {
+      // (a launch that failed to start leaves its error with the runtime)
+      const cudaError_t le = cudaGetLastError();
+      if (le != cudaSuccess) return cuda_fail(le, "neighbour-list pipeline launch");
+      return fail(NLB_ERR_CUDA, "the search ended without its report");
+    }
   }
   std::atomic_thread_fence(std::memory_order_acquire);
   return Status{NLB_OK};
