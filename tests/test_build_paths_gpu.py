@@ -63,3 +63,23 @@ def test_uniform_sizes(nl, oracle, n):
     box = (n / 0.1) ** (1.0 / 3.0)
     pos = rng.uniform(0.0, box, (n, 3))
     check(nl, oracle, pos, box, 5.0, f"uniform {n} rc 5")
+
+
+def test_device_results_past_the_capacity_estimate(nl, oracle):
+    """A dense blob holds far more edges than the density estimate sizes the
+    arrays for: unless earlier builds of the process already grew them, the
+    first launch writes nothing, the arrays grow and the search runs again --
+    here with device results on a caller's stream (the call otherwise returns
+    as soon as M is known)."""
+    import torch
+
+    pos = clustered(4000, 2500, 60.0, 1.5, seed=77)
+    h = np.eye(3) * 60.0
+    cell = nl.PyCell(h.tolist(), [True, True, True])
+    d = torch.from_numpy(np.ascontiguousarray(pos)).cuda()
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        r = nl.build_neighborlists_torch(cell, d, 5.0)
+        got = {"edge_index": r["edge_index"].cpu().numpy(), "shift": r["shift"].cpu().numpy()}
+    ref = oracle.search_single(pos, h, [True, True, True], 5.0, nthreads=8)
+    assert_same(got, ref, "blob, device results")
