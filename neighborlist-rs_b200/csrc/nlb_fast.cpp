@@ -401,7 +401,8 @@ Status run_fast(Ctx& c, SystemPlan& sp, const double* d_pos, int64_t* m_out, boo
     // (M above the capacity: the synchronous path below grows the arrays.)
   }
 
-  // One synchronisation: total edges and the scan's wait-error word.
+  // Without the report (phase profiling, or M above the capacity): one
+  // synchronisation reads the total edges and the scan's wait-error word.
   cudaError_t e = cudaMemcpyAsync(c.h_small, sp.fused ? sp.fused_total : sp.offs + sp.row,
                                   sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream);
   if (e == cudaSuccess)  // the scan's (or the fused look-back's) wait-error word

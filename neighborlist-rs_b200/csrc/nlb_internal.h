@@ -201,7 +201,8 @@ Status count_system(Ctx& c, SystemPlan& sp, const double* d_pos);
 Status emit_system(Ctx& c, SystemPlan& sp, const double* d_pos, const DevLists& L,
                    const int64_t* base, int64_t index_offset);
 
-// Single-cutoff cell-list pipeline with one synchronisation, replayed as a
+// Single-cutoff cell-list pipeline with no host round trip before M is
+// known (the device reports M through host-mapped memory), replayed as a
 // CUDA graph for repeated identical calls (nlb_fast.cpp).  Requires
 // sp.method == kCellList and sp.fp32; leaves the M edges in sp.out_src
 // (sources), sp.out_dst (destinations) and sp.out_sh.  contiguous = true
