@@ -15,8 +15,9 @@ exact-sized edge_index int64 (2, M) and shift int32 (M, 3)).
                (neighborlist_rs.build_neighborlists: numpy positions in, numpy
                edge arrays out), host<->device copies inside the timed region.
 * roofline   : the dominant kernel's algorithmic bytes / its CUDA-event time
-               (the emit pass: the largest share of the ncu launch list; the
-               issue-bound count pass, about as long, is reported beside it).
+               (the one-launch search on the headline's sparse grid; the emit
+               pass, with the count pass beside it, on grids that keep the
+               three launches).
 * cpu_baseline: the CPU oracle (C++ restatement of the reference's rayon
                count/fill path) on the host cores, rank 0, bounded sample.
 * extra      : other configurations (rc 14, isolated N=1000, triclinic
@@ -674,6 +675,7 @@ def extra_measurements(nl, torch, args):
     out["served"] = served_measurements(nl)
     out["output_options_rc6"] = output_option_measurements(nl, torch)
     out["verlet_md_rc6"] = verlet_measurements(nl, torch)
+    out["verlet_md_rc14"] = verlet_measurements(nl, torch, 14.0)
     return out
 
 
@@ -708,8 +710,8 @@ def output_option_measurements(nl, torch):
             "bytes_out_per_edge": 28 + 24 + 8}
 
 
-def verlet_measurements(nl, torch):
-    """MD-style use of the headline system: Verlet list at rc 6 with a 1 A
+def verlet_measurements(nl, torch, rc=6.0):
+    """MD-style use of the headline system: Verlet list at rc with a 1 A
     skin, positions moved by 0.01 A per step (no rebuild inside the sample),
     device positions in, device lists out; against a fresh build per step."""
     from neighborlist_rs.verlet import VerletList
@@ -719,7 +721,7 @@ def verlet_measurements(nl, torch):
     rng = np.random.default_rng(31)
     steps = [torch.from_numpy(pos + rng.normal(0.0, 0.01 / 3 ** 0.5, pos.shape) * (k + 1) / 20)
              .cuda() for k in range(20)]
-    with VerletList(6.0, 1.0) as vl:
+    with VerletList(rc, 1.0) as vl:
         vl.update(cell, steps[0])
         k = [0]
 
@@ -728,9 +730,9 @@ def verlet_measurements(nl, torch):
             k[0] += 1
         t_upd = _median_device_call(torch, one, reps=40, warmup=5)
         st = vl.stats()
-    t_fresh = _median_device_call(torch, lambda: nl.build_neighborlists_torch(cell, steps[5], 6.0))
+    t_fresh = _median_device_call(torch, lambda: nl.build_neighborlists_torch(cell, steps[5], rc))
     return {"update_ms": 1e3 * t_upd, "fresh_build_ms": 1e3 * t_fresh,
-            "stored_edges_rc7": st["stored_edges"], "edges_rc6": st["last_edges"],
+            "stored_edges_rc_plus_skin": st["stored_edges"], "edges": st["last_edges"],
             "rebuilds": st["rebuilds"], "updates": st["updates"]}
 
 

@@ -276,6 +276,11 @@ void nlb_result_ex_free(nlb_result_ex* r);
  *   rebuild).  One synchronisation per update without a rebuild.
  * nlb_verlet_update_device: device positions in; the result arrays are
  *   device pointers owned by the manager, valid until its next update.
+ * nlb_verlet_update_device_owned: as nlb_verlet_update_device, but the two
+ *   result arrays are written in place into blocks of the library's
+ *   stream-ordered result pool and handed over, exactly like
+ *   nlb_build_device_owned's (edge_index [src | dst] in the first 2 M
+ *   entries; return each with nlb_device_free; both NULL when M = 0).
  * nlb_verlet_needs_rebuild: *needs and the current max displacement (+inf
  *   when the next update rebuilds anyway); positions_on_device selects the
  *   pointer kind.
@@ -288,6 +293,9 @@ int nlb_verlet_update(nlb_verlet* v, const double* positions, int64_t n_atoms, c
 int nlb_verlet_update_device(nlb_verlet* v, const double* d_positions, int64_t n_atoms,
                              const double* cell, const uint8_t* pbc, int* rebuilt,
                              nlb_device_result* out);
+int nlb_verlet_update_device_owned(nlb_verlet* v, const double* d_positions, int64_t n_atoms,
+                                   const double* cell, const uint8_t* pbc, int* rebuilt,
+                                   nlb_device_result* out);
 int nlb_verlet_needs_rebuild(nlb_verlet* v, const double* positions, int64_t n_atoms,
                              const double* cell, const uint8_t* pbc, int positions_on_device,
                              int* needs, double* max_displacement);

@@ -353,6 +353,31 @@ void take_result_arrays(Ctx& c, int64_t** ei, int32_t** sh) {
   *bs[1] = Ctx::Buf{};
 }
 
+void* alloc_owned_device(int device, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool = result_pool_for(device);
+  void* p = nullptr;
+  if (!pool || cudaMallocFromPoolAsync(&p, std::max<size_t>(bytes, 256), pool, s) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  ResultPool& rp = result_pool();
+  std::lock_guard<std::mutex> lk(rp.mu);
+  rp.owned[p] = {device, bytes};
+  ++rp.handed;
+  return p;
+}
+
+void release_owned_device(void* p, cudaStream_t s) {
+  if (!p) return;
+  ResultPool& rp = result_pool();
+  {
+    std::lock_guard<std::mutex> lk(rp.mu);
+    if (rp.owned.erase(p) == 0) return;
+    ++rp.returned;
+  }
+  cudaFreeAsync(p, s);
+}
+
 void* Ctx::raw(int slot, size_t bytes) {
   Buf& b = bufs[slot];
   if (bytes > b.cap && is_result_slot(slot)) {

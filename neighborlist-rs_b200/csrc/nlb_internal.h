@@ -132,6 +132,12 @@ void take_result_arrays(Ctx& c, int64_t** ei, int32_t** sh);
 // Frees the calling thread's contexts and fast-path graphs (threads that end
 // before the process does, e.g. server workers).
 void release_thread_ctx();
+// A device block of the per-device stream-ordered result pool, allocated on
+// stream s and registered as handed to a caller (nlb_device_free returns
+// it); nullptr on failure.  release_owned_device takes one back that was
+// never handed over after all.
+void* alloc_owned_device(int device, size_t bytes, cudaStream_t s);
+void release_owned_device(void* p, cudaStream_t s);
 void release_fast_states();
 void release_batch_graphs();
 // Counts CUDA-graph replays of the fast paths (nlb_graph_replays).

@@ -358,14 +358,18 @@ void launch_edge_extras(const double* pos, const EdgeExtrasCell& cell, const int
                         int32_t* sh_out, double* vec, double* dist, cudaStream_t s);
 
 // Verlet list manager (k_verlet.cu): largest squared displacement against
-// the reference positions (as the bits of a double in *out); keep flags of
-// the stored edges at rc; compaction of the kept edges in stored order.
+// the reference positions (as the bits of a double in *out); the stored
+// edges kept at rc, compacted in stored order.
 void launch_max_disp(const double* pos, const double* ref, int64_t n, unsigned long long* out,
                      cudaStream_t s);
-void launch_verlet_keep(const double* pos, const EdgeExtrasCell& cell, const int64_t* ei,
-                        const int32_t* sh, int64_t m, double rc_sq, uint32_t* keep,
-                        cudaStream_t s);
-void launch_verlet_emit(const int64_t* ei, const int32_t* sh, int64_t m, const uint32_t* keep,
-                        const int64_t* offs, int64_t* out_ei, int32_t* out_sh, cudaStream_t s);
+// The kept edges in one pass (k_verlet_compact): out_ei [src | dst] of M
+// edges and out_sh; dst_tmp has room for m destinations; state has
+// verlet_compact_state_words(m) words (cleared here): [1] the look-back's
+// error word, [3] M.
+int64_t verlet_compact_state_words(int64_t m);
+void launch_verlet_compact(const double* pos, const EdgeExtrasCell& cell, const int64_t* ei,
+                           const int32_t* sh, int64_t m, double rc_sq, int64_t* out_ei,
+                           int32_t* out_sh, int64_t* dst_tmp, uint64_t* state,
+                           int32_t spin_limit, cudaStream_t s);
 
 }  // namespace nlb

@@ -29,6 +29,9 @@
 
 namespace nlb {
 
+// Polls of one look-back wait in the Verlet compaction before it gives up.
+constexpr int32_t kVerletSpinLimit = 1 << 22;
+
 // Search pieces shared with nlb_api.cpp.
 Status half_list_device(Ctx& c, const double* pos_host, const double* d_pos, int64_t n,
                         const double* cell9, const uint8_t* pbc, double cutoff, int64_t** ei,
@@ -69,7 +72,7 @@ class Verlet {
   // first.  Results stay in the manager's buffers until the next update.
   Status update(const double* pos_host, const double* d_pos_in, int64_t n, const double* cell9,
                 const uint8_t* pbc, int* rebuilt, int64_t* m_out, int64_t** ei_out,
-                int32_t** sh_out) {
+                int32_t** sh_out, bool owned = false) {
     std::lock_guard<std::mutex> lk(mu_);
     *rebuilt = 0;
     *m_out = 0;
@@ -92,11 +95,33 @@ class Verlet {
     ++updates_;
     bool rebuild = !same_system(n, cell9, pbc);
     if (!rebuild && n > 0) {
-      double d2 = 0.0;
-      st = max_disp_sq(*c, d_pos, n, &d2);
+      // The displacement check and the filter of the stored list go out
+      // together (the filter only reads the positions and the list) and one
+      // synchronisation reads both; a rebuild, when due, discards the filter.
+      auto* d = static_cast<unsigned long long*>(disp_.get(sizeof(unsigned long long)));
+      if (!d) return fail(NLB_ERR_NOMEM, "device allocation failed");
+      launch_max_disp(d_pos, static_cast<const double*>(ref_.p), n, d, s);
+      cudaError_t e = cudaMemcpyAsync(c->h_small + 2, d, sizeof(unsigned long long),
+                                      cudaMemcpyDeviceToHost, s);
+      if (e != cudaSuccess) return cuda_fail(e, "displacement check");
+      st = filter(*c, d_pos, m_out, ei_out, sh_out, owned);
       if (!st.ok()) return st;
+      if (m_list_ == 0) {  // (the filter had nothing to do and did not synchronise)
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_fail(e, "displacement check");
+      }
+      double d2 = 0.0;
+      std::memcpy(&d2, c->h_small + 2, sizeof(double));
       last_disp_ = std::sqrt(d2);
       rebuild = last_disp_ > 0.5 * skin_;
+      if (!rebuild) return Status{NLB_OK};
+      if (owned) {
+        release_owned_device(*ei_out, s);
+        release_owned_device(*sh_out, s);
+      }
+      *m_out = 0;
+      *ei_out = nullptr;
+      *sh_out = nullptr;
     }
     if (rebuild) {
       st = rebuild_list(*c, pos_host, d_pos, n, cell9, pbc);
@@ -107,7 +132,7 @@ class Verlet {
       *rebuilt = 1;
       ++rebuilds_;
     }
-    return filter(*c, d_pos, m_out, ei_out, sh_out);
+    return filter(*c, d_pos, m_out, ei_out, sh_out, owned);
   }
 
   // Largest displacement since the last rebuild (+inf when there is no list
@@ -213,16 +238,38 @@ class Verlet {
     return Status{NLB_OK};
   }
 
+  // owned: the kept edges go to blocks of the result pool sized for the
+  // whole stored list, handed to the caller (released again on failure).
   Status filter(Ctx& c, const double* d_pos, int64_t* m_out, int64_t** ei_out,
-                int32_t** sh_out) {
+                int32_t** sh_out, bool owned = false) {
     const int64_t m = m_list_;
-    int64_t* out_ei = static_cast<int64_t*>(out_ei_.get(16 * (size_t)m));
-    int32_t* out_sh = static_cast<int32_t*>(out_sh_.get(12 * (size_t)m));
-    uint32_t* keep = static_cast<uint32_t*>(keep_.get(4 * (size_t)m));
-    int64_t* offs = static_cast<int64_t*>(offs_.get(8 * (size_t)(m + 1)));
-    int64_t* tmp = static_cast<int64_t*>(scan_tmp_.get(8 * (size_t)scan_tmp_elems(m)));
-    if (!out_ei || !out_sh || !keep || !offs || !tmp)
+    int64_t* out_ei = nullptr;
+    int32_t* out_sh = nullptr;
+    if (owned) {
+      if (m > 0) {
+        out_ei = static_cast<int64_t*>(alloc_owned_device(c.device, 16 * (size_t)m, c.stream));
+        out_sh = static_cast<int32_t*>(alloc_owned_device(c.device, 12 * (size_t)m, c.stream));
+        if (!out_ei || !out_sh) {
+          release_owned_device(out_ei, c.stream);
+          release_owned_device(out_sh, c.stream);
+          return fail(NLB_ERR_NOMEM, "device allocation failed");
+        }
+      }
+    } else {
+      out_ei = static_cast<int64_t*>(out_ei_.get(16 * (size_t)m));
+      out_sh = static_cast<int32_t*>(out_sh_.get(12 * (size_t)m));
+      if (!out_ei || !out_sh) return fail(NLB_ERR_NOMEM, "device allocation failed");
+    }
+    int64_t* dst_tmp = static_cast<int64_t*>(dst_tmp_.get(8 * (size_t)m));
+    uint64_t* state =
+        static_cast<uint64_t*>(state_.get(8 * (size_t)verlet_compact_state_words(m)));
+    if (!dst_tmp || !state) {
+      if (owned) {
+        release_owned_device(out_ei, c.stream);
+        release_owned_device(out_sh, c.stream);
+      }
       return fail(NLB_ERR_NOMEM, "device allocation failed");
+    }
     *ei_out = out_ei;
     *sh_out = out_sh;
     if (m == 0) {
@@ -236,17 +283,25 @@ class Verlet {
     }
     const int64_t* vei = static_cast<const int64_t*>(list_ei_.p);
     const int32_t* vsh = static_cast<const int32_t*>(list_sh_.p);
-    launch_verlet_keep(d_pos, cell, vei, vsh, m, rc_ * rc_, keep, c.stream);
-    exclusive_scan_u32(keep, m, offs, tmp, c.stream);
-    launch_verlet_emit(vei, vsh, m, keep, offs, out_ei, out_sh, c.stream);
-    cudaError_t e = cudaMemcpyAsync(c.h_small, offs + m, sizeof(int64_t), cudaMemcpyDeviceToHost,
+    launch_verlet_compact(d_pos, cell, vei, vsh, m, rc_ * rc_, out_ei, out_sh, dst_tmp, state,
+                          kVerletSpinLimit, c.stream);
+    // M and the look-back's bounded-wait error word
+    cudaError_t e = cudaMemcpyAsync(c.h_small, state + 3, sizeof(int64_t), cudaMemcpyDeviceToHost,
                                     c.stream);
-    if (e == cudaSuccess)  // the scan's bounded-wait error word
-      e = cudaMemcpyAsync(c.h_small + 1, tmp + 1, sizeof(int64_t), cudaMemcpyDeviceToHost,
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c.h_small + 1, state + 1, sizeof(int64_t), cudaMemcpyDeviceToHost,
                           c.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
-    if (e != cudaSuccess) return cuda_fail(e, "Verlet filter");
-    if (c.h_small[1] != 0) return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+    if (e != cudaSuccess || c.h_small[1] != 0) {
+      if (owned) {
+        release_owned_device(out_ei, c.stream);
+        release_owned_device(out_sh, c.stream);
+        *ei_out = nullptr;
+        *sh_out = nullptr;
+      }
+      if (e != cudaSuccess) return cuda_fail(e, "Verlet filter");
+      return fail(NLB_ERR_CUDA, "prefix scan gave up waiting for a tile");
+    }
     m_last_ = c.h_small[0];
     *m_out = m_last_;
     return Status{NLB_OK};
@@ -262,7 +317,7 @@ class Verlet {
   int64_t m_list_ = 0, m_last_ = 0;
   int64_t updates_ = 0, rebuilds_ = 0;
   double last_disp_ = 0.0;
-  DevBuf pos_up_, ref_, disp_, list_ei_, list_sh_, out_ei_, out_sh_, keep_, offs_, scan_tmp_;
+  DevBuf pos_up_, ref_, disp_, list_ei_, list_sh_, out_ei_, out_sh_, dst_tmp_, state_;
 };
 
 }  // namespace nlb
@@ -337,6 +392,36 @@ int nlb_verlet_update_device(nlb_verlet* v, const double* d_positions, int64_t n
   nlb::Status st = v->impl->update(nullptr, d_positions ? d_positions : &kNone, n_atoms, cell,
                                    pbc, rebuilt, &m, &ei, &sh);
   if (!st.ok()) return st.code;
+  out->n_edges = m;
+  out->edge_index = ei;
+  out->shift = sh;
+  return NLB_OK;
+}
+
+int nlb_verlet_update_device_owned(nlb_verlet* v, const double* d_positions, int64_t n_atoms,
+                                   const double* cell, const uint8_t* pbc, int* rebuilt,
+                                   nlb_device_result* out) {
+  if (!v || !out || !rebuilt) return nlb::fail(NLB_ERR_VALUE, "NULL argument").code;
+  out->n_edges = 0;
+  out->edge_index = nullptr;
+  out->shift = nullptr;
+  if (n_atoms > 0 && !d_positions) return nlb::fail(NLB_ERR_VALUE, "positions is NULL").code;
+  int64_t m = 0;
+  int64_t* ei = nullptr;
+  int32_t* sh = nullptr;
+  static const double kNone = 0.0;
+  nlb::Status st = v->impl->update(nullptr, d_positions ? d_positions : &kNone, n_atoms, cell,
+                                   pbc, rebuilt, &m, &ei, &sh, true);
+  if (!st.ok()) return st.code;
+  if (m == 0) {
+    // (blocks sized for a non-empty stored list, but nothing was kept)
+    nlb::Ctx* c = nullptr;
+    if (nlb::get_ctx(&c).ok()) {
+      nlb::release_owned_device(ei, c->stream);
+      nlb::release_owned_device(sh, c->stream);
+    }
+    return NLB_OK;
+  }
   out->n_edges = m;
   out->edge_index = ei;
   out->shift = sh;

@@ -20,7 +20,7 @@ from __future__ import annotations
 
 import ctypes
 
-from . import (_DevResult, _Result, _cell_args, _check, _check_cutoff, _cudart_copy, _dp, _lib,
+from . import (_DeviceBlock, _DevResult, _Result, _cell_args, _check, _check_cutoff, _dp, _lib,
                _positions, _to_dict, _u8p)
 
 _lib.nlb_verlet_create.argtypes = [ctypes.c_double, ctypes.c_double]
@@ -30,6 +30,9 @@ _lib.nlb_verlet_update.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int64, _dp, _u
 _lib.nlb_verlet_update_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _dp,
                                           _u8p, ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(_DevResult)]
+_lib.nlb_verlet_update_device_owned.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                                _dp, _u8p, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(_DevResult)]
 _lib.nlb_verlet_needs_rebuild.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _dp,
                                           _u8p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_double)]
@@ -67,8 +70,10 @@ class VerletList:
     def update(self, cell, positions):
         """Pairs within the cutoff for these positions: numpy (N, 3) float64
         in -> build_neighborlists dict; CUDA float64 tensor in -> the same
-        dict of CUDA tensors (copied out of the manager's buffers on the
-        current torch stream)."""
+        dict of CUDA tensors, produced on the current torch stream: the
+        library's result blocks themselves (written in place, handed over,
+        returned to the pool when the tensors are freed), as in
+        build_neighborlists_torch."""
         h, pb = _cell_args(cell)
         flag = ctypes.c_int(0)
         if _is_cuda_tensor(positions):
@@ -87,17 +92,20 @@ class VerletList:
                 set_stream(stream.cuda_stream)
                 try:
                     r = _DevResult()
-                    _check(_lib.nlb_verlet_update_device(
+                    _check(_lib.nlb_verlet_update_device_owned(
                         self._handle(), ctypes.c_void_p(pos.data_ptr()), pos.shape[0], h, pb,
                         ctypes.byref(flag), ctypes.byref(r)))
-                    m = int(r.n_edges)
-                    ei = torch.empty((2, m), dtype=torch.int64, device=dev)
-                    sh = torch.empty((m, 3), dtype=torch.int32, device=dev)
-                    if m:
-                        _cudart_copy(ei.data_ptr(), r.edge_index, 16 * m, stream.cuda_stream)
-                        _cudart_copy(sh.data_ptr(), r.shift, 12 * m, stream.cuda_stream)
                 finally:
                     set_stream(None)
+                m = int(r.n_edges)
+                if m == 0:
+                    ei = torch.zeros((2, 0), dtype=torch.int64, device=dev)
+                    sh = torch.zeros((0, 3), dtype=torch.int32, device=dev)
+                else:
+                    ei = torch.as_tensor(_DeviceBlock(r.edge_index, (2, m), "<i8",
+                                                      stream.cuda_stream), device=dev)
+                    sh = torch.as_tensor(_DeviceBlock(r.shift, (m, 3), "<i4",
+                                                      stream.cuda_stream), device=dev)
             self.rebuilt = bool(flag.value)
             return {"edge_index": ei, "shift": sh}
         pos = _positions(positions)

@@ -174,3 +174,36 @@ def test_verlet_matches_oracle_restatement(nl, oracle, kind):
             want = oracle.verlet_filter(pos, h, stored, rc)
             assert_same(res, want, f"{kind} step {k}")
     assert reused >= 1
+
+
+def test_verlet_device_results_are_library_blocks(nl):
+    """Device updates hand over the blocks the compaction wrote (no copy):
+    two blocks per update with edges, returned to the pool when the tensors
+    go; the lists equal the host update's."""
+    import gc
+
+    import torch
+
+    from neighborlist_rs import workloads as W
+    from neighborlist_rs.verlet import VerletList
+
+    pos, rows = W.cluster_liquid(n_clusters=400, box=33.0, seed=5)
+    cell = nl.PyCell(rows.T.tolist())
+    rng = np.random.default_rng(8)
+    gc.collect()
+    b0 = nl.device_blocks()
+    with VerletList(6.0, 1.0) as vd, VerletList(6.0, 1.0) as vh:
+        for k in range(4):
+            p = pos + rng.normal(0.0, 0.02, pos.shape) * k
+            rd = vd.update(cell, torch.from_numpy(p).cuda())
+            rh = vh.update(cell, p)
+            assert np.array_equal(rd["edge_index"].cpu().numpy(), rh["edge_index"])
+            assert np.array_equal(rd["shift"].cpu().numpy(), rh["shift"])
+            assert rd["edge_index"].shape[1] > 0
+            b1 = nl.device_blocks()
+            assert b1["handed"] - b0["handed"] >= 2 * (k + 1)
+            del rd
+            gc.collect()
+    torch.cuda.synchronize()
+    b2 = nl.device_blocks()
+    assert b2["returned"] - b0["returned"] == b2["handed"] - b0["handed"]
