@@ -12,6 +12,7 @@
 // gathers per stored edge and 28 B (+ 16 for the destinations' move) per
 // kept edge).
 #include <algorithm>
+#include <atomic>
 
 #include "nlb_kernels.h"
 
@@ -240,11 +241,22 @@ void launch_verlet_compact(const double* pos, const EdgeExtrasCell& cell, const 
                            int32_t spin_limit, cudaStream_t s) {
   cudaMemsetAsync(state, 0, sizeof(uint64_t) * (size_t)verlet_compact_state_words(m), s);
   if (m <= 0) return;
-  int dev = 0, sms = 0, per_sm = 0;
+  // (SMs and resident CTAs per SM of each device, looked up once)
+  static std::atomic<int> cached[64][2];
+  int dev = 0;
   cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_verlet_compact, kVcThreads, 0);
-  if (per_sm < 1) per_sm = 1;
+  const bool known = dev >= 0 && dev < 64;
+  int sms = known ? cached[dev][0].load() : 0, per_sm = known ? cached[dev][1].load() : 0;
+  if (sms <= 0 || per_sm <= 0) {
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_verlet_compact, kVcThreads, 0);
+    sms = std::max(sms, 1);
+    per_sm = std::max(per_sm, 1);
+    if (known) {
+      cached[dev][0].store(sms);
+      cached[dev][1].store(per_sm);
+    }
+  }
   const int64_t n_tiles = (m + kVcTile - 1) / kVcTile;
   const int64_t grid = std::min<int64_t>((int64_t)sms * per_sm, std::max<int64_t>(n_tiles, sms));
   k_verlet_compact<<<(unsigned)grid, kVcThreads, 0, s>>>(pos, cell, ei, sh, m, rc_sq, out_ei,
