@@ -183,7 +183,8 @@ __global__ void k_plan(const double* __restrict__ pos, const int64_t* __restrict
 
 struct SmemView {
   uint64_t* bcode;  // [cap] sort key 1 (bin Morton code), sorted
-  uint64_t* key;    // [cap] sort key 2 (atom Morton key)
+  uint64_t* key;    // [cap] sort key 2 (atom Morton key); after the sort, the
+                    // boxes of the 32-slot blocks (6 doubles each: cap >= 32)
   int32_t* idx;     // [cap] sort key 3 (local atom index)
   double* px;       // [cap] wrapped (cell list) or raw (brute) positions
   double* py;
@@ -284,6 +285,60 @@ __device__ void load_system(const SysPlan& P, const double* __restrict__ pos, co
     v.meta[p] = m;
   }
   __syncthreads();
+  // FP64 bounding box of each aligned block of 32 sorted slots (blocks are
+  // Morton-contiguous, so the boxes are tight); a block with a non-finite
+  // coordinate gets the infinite box (never pruned).
+  double* box = reinterpret_cast<double*>(v.key);
+  const int lane = threadIdx.x & 31;
+  for (int a = threadIdx.x >> 5; a < (n + 31) >> 5; a += blockDim.x >> 5) {
+    const int p = 32 * a + lane;
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    bool bad = false;
+    if (p < n) {
+      const double c[3] = {v.px[p], v.py[p], v.pz[p]};
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = hi[k] = c[k];
+        bad = bad || !isfinite(c[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      for (int o = 16; o > 0; o >>= 1) {
+        const double l2 = __shfl_xor_sync(0xffffffffu, lo[k], o);
+        const double h2 = __shfl_xor_sync(0xffffffffu, hi[k], o);
+        lo[k] = l2 < lo[k] ? l2 : lo[k];
+        hi[k] = h2 > hi[k] ? h2 : hi[k];
+      }
+    if (__any_sync(0xffffffffu, bad))
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = -INFINITY;
+        hi[k] = INFINITY;
+      }
+    if (lane < 6) box[6 * a + lane] = lane < 3 ? lo[lane] : hi[lane - 3];
+  }
+  __syncthreads();
+}
+
+// Whether the block's box may hold a candidate within the cutoff of the
+// atom at t = (atom - image offset): the box distance, shortened per axis by
+// a slack far above the rounding of the pair test's own differences, against
+// max_sq (1 + 1e-12).  Only removes candidates that cannot hit.
+__device__ __forceinline__ bool block_near(const double* __restrict__ box, int a, const double* t,
+                                           double thr) {
+  const double* B = box + 6 * a;
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double lo = B[k], hi = B[3 + k];
+    double d = dsub(lo, t[k]);
+    const double d2 = dsub(t[k], hi);
+    d = d2 > d ? d2 : d;
+    const double slack = dmul(1e-14, dadd(fabs(t[k]), fmax(fabs(lo), fabs(hi))));
+    d = d > slack ? dsub(d, slack) : 0.0;
+    s = dadd(s, dmul(d, d));
+  }
+  return !(s > thr);
 }
 
 // First index in [0, n) whose code is >= c.
@@ -317,10 +372,13 @@ __device__ __forceinline__ void visit_smem_grid_atom(const SysPlan& P, const Sme
   }
   const int32_t ny = 2 * g.ns[1] + 1, nz = 2 * g.ns[2] + 1;
   const int64_t n_cells = (int64_t)(2 * g.ns[0] + 1) * ny * nz;
+  const double* box = reinterpret_cast<const double*>(v.key);
+  const double thr = dmul(max_sq, 1.0 + 1e-12);
   for (int64_t c0 = 0; c0 < n_cells; c0 += 32) {
     const int64_t c = c0 + lane;
     bool ok = c < n_cells;
     int b0 = 0, b1 = 0;
+    uint32_t cmask = 0;
     double off[3] = {0.0, 0.0, 0.0};
     int32_t sh[3] = {0, 0, 0};
     if (ok) {
@@ -344,10 +402,30 @@ __device__ __forceinline__ void visit_smem_grid_atom(const SysPlan& P, const Sme
       if (norm2(dsub(cs[0], pix), dsub(cs[1], piy), dsub(cs[2], piz)) > g.prune_sq) {
         ok = false;
       } else {
-        const uint64_t code = bin_code(bin[0], bin[1], bin[2]);
-        b0 = lower_bound_code(v.bcode, n, code);
-        b1 = code == ~0ull ? n : lower_bound_code(v.bcode, n, code + 1);
+        if (g.total_bins == 1) {  // (one bin: every image cell holds all the atoms)
+          b0 = 0;
+          b1 = n;
+        } else {
+          const uint64_t code = bin_code(bin[0], bin[1], bin[2]);
+          b0 = lower_bound_code(v.bcode, n, code);
+          b1 = code == ~0ull ? n : lower_bound_code(v.bcode, n, code + 1);
+        }
         ok = b1 > b0;
+        if (ok) {
+          // Candidate chunks [b0 + 32k, ...) of this cell whose slots' block
+          // boxes may hold a hit (chunks from the 33rd on are always kept).
+          const double t[3] = {dsub(pix, off[0]), dsub(piy, off[1]), dsub(piz, off[2])};
+          const int nch = (b1 - b0 + 31) >> 5;
+          const int lim = nch < 32 ? nch : 32;
+          for (int k = 0; k < lim; ++k) {
+            const int f = b0 + 32 * k;
+            const int l = (f + 32 < b1 ? f + 32 : b1) - 1;
+            if (block_near(box, f >> 5, t, thr) ||
+                ((l >> 5) != (f >> 5) && block_near(box, l >> 5, t, thr)))
+              cmask |= 1u << k;
+          }
+          ok = cmask != 0 || nch > 32;
+        }
       }
     }
     unsigned cells = __ballot_sync(0xffffffffu, ok);
@@ -362,7 +440,9 @@ __device__ __forceinline__ void visit_smem_grid_atom(const SysPlan& P, const Sme
       cshift[1] = __shfl_sync(0xffffffffu, sh[1], src);
       cshift[2] = __shfl_sync(0xffffffffu, sh[2], src);
       const bool shifted = (cshift[0] | cshift[1] | cshift[2]) != 0;
-      for (int jb = j0; jb < j1; jb += 32) {
+      const uint32_t ck = __shfl_sync(0xffffffffu, cmask, src);
+      for (int jb = j0, k = 0; jb < j1; jb += 32, ++k) {
+        if (k < 32 && !((ck >> k) & 1u)) continue;
         sink.at(jb, cshift);
         const int j = jb + lane;
         bool hit = false;
@@ -460,8 +540,12 @@ __device__ __forceinline__ void system_cutoff(const CutoffSet& cs, const SysPlan
 // fields}.  Lane l buffers the atom's l-th pending record; 32 pending
 // records (and the atom's last ones) are flushed as one segment whose header
 // holds the atom's run slot, its edges in earlier segments, the record count
-// and the system.  A segment or a shift that does not fit sets the overflow
-// flag: the emit pass then recomputes instead of expanding.
+// and the system.  Each atom's first segment was reserved with its warp's
+// other atoms of the work item (one atomic per warp and item: a global
+// atomic per atom serialised the pass on the counter); it is written even
+// when empty, and further segments (atoms with more than 32 records) are
+// taken one by one.  A segment or a shift that does not fit sets the
+// overflow flag: the emit pass then recomputes instead of expanding.
 struct RecSink {
   const CutoffSet* cs;
   BatchRecords rb;
@@ -469,6 +553,7 @@ struct RecSink {
   uint32_t r_mask = 0, r_j = 0, r_sh = 0;  // lane l: pending record l
   int n_rec = 0, e_done = 0, e_buf = 0;  // warp-uniform
   int32_t p_abs = 0, sys = 0;
+  int first_sg = -1;  // the atom's reserved segment (-1: used)
   uint32_t cur_j = 0, cur_sh = 0;
   bool sh_ok = true;
 
@@ -479,12 +564,16 @@ struct RecSink {
     cur_sh = ((uint32_t)csh[0] & 1023u) | (((uint32_t)csh[1] & 1023u) << 10) |
              (((uint32_t)csh[2] & 1023u) << 20);
   }
-  __device__ __forceinline__ void flush() {
-    if (n_rec == 0) return;
+  __device__ __forceinline__ void flush(bool last) {
+    if (n_rec == 0 && !(last && first_sg >= 0)) return;
     const int lane = threadIdx.x & 31;
-    int sg = 0;
-    if (lane == 0) sg = atomicAdd(rb.seg_top, 1);
-    sg = __shfl_sync(0xffffffffu, sg, 0);
+    int sg = first_sg;
+    if (sg >= 0) {
+      first_sg = -1;
+    } else {
+      if (lane == 0) sg = atomicAdd(rb.seg_top, 1);
+      sg = __shfl_sync(0xffffffffu, sg, 0);
+    }
     if (sg < rb.seg_cap) {
       if (lane < n_rec) {
         uint32_t* r = rb.rec + ((size_t)sg * 32 + lane) * 3;
@@ -515,7 +604,7 @@ struct RecSink {
     }
     ++n_rec;
     e_buf += __popc(m);
-    if (n_rec == 32) flush();
+    if (n_rec == 32) flush(false);
   }
 };
 
@@ -556,16 +645,24 @@ __global__ void __launch_bounds__(THREADS, THREADS >= 512 ? 1 : 768 / THREADS)
         rb.meta[P.slot + p] = m;
       }
     }
-    for (int p = item.y + warp; p < p_end; p += kWarps) {
+    // (REC: this warp's atoms of the item reserve their first segments)
+    int seg_base = 0;
+    if (REC) {
+      const int mine = p_end - item.y > warp ? (p_end - item.y - warp + kWarps - 1) / kWarps : 0;
+      if (lane == 0 && mine > 0) seg_base = atomicAdd(rb.seg_top, mine);
+      seg_base = __shfl_sync(0xffffffffu, seg_base, 0);
+    }
+    for (int p = item.y + warp, q = 0; p < p_end; p += kWarps, ++q) {
       if (REC) {
         RecSink sink{csp, rb};
         sink.p_abs = P.slot + p;
         sink.sys = item.x;
+        sink.first_sg = seg_base + q;
         if (P.method == 2)
           visit_smem_grid_atom(P, v, p, csp->max_sq, sink);
         else
           visit_smem_brute_atom(P, v, p, csp->max_sq, sink);
-        sink.flush();
+        sink.flush(true);
         if (lane == 0) counts[P.slot + p] = sink.cnt;
       } else {
         CountSink sink{csp, 0u};
