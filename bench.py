@@ -881,8 +881,13 @@ def served_measurements(nl):
     full_dist = as_reqs(W.request_stream(600, seed=23))
     res = {}
     with Server(hbm_budget_bytes=40 << 30, workers=4, max_batch=4096) as srv:
-        run_stream_raw(srv, full_dist[:200], device=True)
-        run_stream(srv, full_dist[:200], None, device=True)
+        # Untimed passes over every request first: a worker grows its
+        # workspace (a device-synchronising reallocation of up to several
+        # GB) the first time it meets a larger request, a one-time cost per
+        # worker that would otherwise land in whichever timed run meets it.
+        run_stream_raw(srv, full_dist, device=True)
+        run_stream(srv, full_dist, None, device=True)
+        run_stream(srv, full_dist, 2000, seed=1, device=True)
         for rate in (500, 1000, 2000):
             res[f"poisson_{rate}_device"] = run_stream(srv, full_dist, rate, seed=rate, device=True)
         run_stream(srv, full_dist[:100], None)
