@@ -333,8 +333,6 @@ cudaMemPool_t result_pool_for(int dev) {
   return rp.pool[dev];
 }
 
-bool is_result_slot(int slot) { return slot == kSlotOutEi || slot == kSlotOutSh; }
-
 }  // namespace
 
 void take_result_arrays(Ctx& c, int64_t** ei, int32_t** sh) {
@@ -380,10 +378,13 @@ void release_owned_device(void* p, cudaStream_t s) {
 
 void* Ctx::raw(int slot, size_t bytes) {
   Buf& b = bufs[slot];
-  if (bytes > b.cap && is_result_slot(slot)) {
-    // Result arrays come from the stream-ordered pool.  Growth waits for the
-    // device first (the old array may still be in use on another stream, as
-    // a cudaFree would).
+  if (bytes > b.cap) {
+    // Every slot comes from the stream-ordered pool (result arrays must, to
+    // be handed over; the others so that a grown slot's old memory stays
+    // mapped for the next allocation instead of being unmapped by cudaFree
+    // and mapped again by cudaMalloc).  Growth waits for the device first
+    // (the old array may still be in use on another stream, as a cudaFree
+    // would).
     if (b.p) {
       cudaDeviceSynchronize();
       if (b.pooled)
@@ -402,18 +403,6 @@ void* Ctx::raw(int slot, size_t bytes) {
     b.cap = cap;
     b.pooled = true;
     return b.p;
-  }
-  if (bytes > b.cap) {
-    if (b.p) cudaFree(b.p);
-    b.p = nullptr;
-    b.cap = 0;
-    size_t cap = std::max<size_t>(bytes + bytes / 4, 4096);
-    if (cudaMalloc(&b.p, cap) != cudaSuccess) {
-      cudaGetLastError();
-      b.p = nullptr;
-      return nullptr;
-    }
-    b.cap = cap;
   }
   return b.p;
 }
