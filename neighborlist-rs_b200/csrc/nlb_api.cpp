@@ -351,6 +351,16 @@ void take_result_arrays(Ctx& c, int64_t** ei, int32_t** sh) {
   *bs[1] = Ctx::Buf{};
 }
 
+void warm_result_pool(int device, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool = result_pool_for(device);
+  void* p = nullptr;
+  if (pool && bytes > 0 && cudaMallocFromPoolAsync(&p, bytes, pool, s) == cudaSuccess) {
+    cudaFreeAsync(p, s);
+    cudaStreamSynchronize(s);
+  }
+  cudaGetLastError();
+}
+
 void* alloc_owned_device(int device, size_t bytes, cudaStream_t s) {
   cudaMemPool_t pool = result_pool_for(device);
   void* p = nullptr;

@@ -137,6 +137,12 @@ void release_thread_ctx();
 // it); nullptr on failure.  release_owned_device takes one back that was
 // never handed over after all.
 void* alloc_owned_device(int device, size_t bytes, cudaStream_t s);
+// Maps `bytes` of the device's stream-ordered pool (the one every workspace
+// slot and result array comes from) now and leaves them free in it: later
+// growth of a thread's workspace takes them without mapping device memory on
+// its critical path.  The pool keeps them mapped (release threshold:
+// unlimited).
+void warm_result_pool(int device, size_t bytes, cudaStream_t s);
 void release_owned_device(void* p, cudaStream_t s);
 void release_fast_states();
 void release_batch_graphs();

@@ -77,6 +77,8 @@ constexpr size_t kReservePinnedMin = size_t(1) << 30;
 constexpr size_t kReservePinnedMax = size_t(4) << 30;
 // Device-result pool memory mapped when a server starts (at most its budget).
 constexpr size_t kPoolWarm = size_t(8) << 30;
+// Workspace memory mapped at start (at most a quarter of the budget).
+constexpr size_t kWorkspaceWarm = size_t(16) << 30;
 
 // Pinned block size for `bytes`: the next power of two (at least 1 MB), so
 // blocks of consecutive batches are interchangeable in the pool.
@@ -157,6 +159,10 @@ class Server {
       cudaStreamSynchronize(free_stream_);
     }
     cudaGetLastError();
+    // The same for the pool the workers' workspaces grow from: a worker
+    // that first meets a request larger than any it has held maps several
+    // GB (result arrays, hit masks) while the others wait.
+    warm_result_pool(device_, std::min<size_t>(budget_ / 4, kWorkspaceWarm), free_stream_);
     // Pinned host blocks for request positions and host results, carved
     // before the first request rather than on its critical path.
     pinned_reserve(std::min(kReservePinnedMax, std::max(kReservePinnedMin, budget_ / 8)));
