@@ -16,7 +16,10 @@
  * Every function returns NLB_OK or an error code; nlb_last_error() gives the
  * calling thread's last message (the reference's Err(String) texts).
  * All entry points are thread-safe: each host thread gets its own CUDA stream
- * and device workspace on the current device.
+ * and device workspace on the current device.  Workspaces and result arrays
+ * come from one stream-ordered memory pool per device, which keeps the
+ * memory it has mapped for the life of the process (a thread's workspace
+ * goes back to the pool, not to the driver, when the thread ends).
  */
 #ifndef NEIGHBORLIST_B200_H
 #define NEIGHBORLIST_B200_H
@@ -366,9 +369,11 @@ int nlb_build_noalloc(const double* d_positions, int64_t n_atoms, double cutoff,
  *   any batch holding this queued request fails as if a CUDA call had
  *   returned an error; the worker reruns that batch one request at a time,
  *   so only this request fails (NLB_ERR_CUDA) and the others complete.
+ * nlb_server_create also maps a quarter of the budget (at most 16 GB) of
+ *   the workspace pool, so that workers grow into mapped memory.
  * nlb_server_destroy: cancels queued requests, lets running ones finish,
- *   joins the workers (freeing their workspaces) and frees every result that
- *   was not handed over.  No thread may be inside nlb_server_wait then. */
+ *   joins the workers (returning their workspaces to the pool) and frees
+ *   every result that was not handed over.  No thread may be inside nlb_server_wait then. */
 typedef struct nlb_server nlb_server;
 nlb_server* nlb_server_create(int device, int64_t hbm_budget_bytes, int n_workers, int max_batch);
 int64_t nlb_server_submit(nlb_server* server, const double* positions, int64_t n_atoms,
