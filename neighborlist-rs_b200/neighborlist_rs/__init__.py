@@ -600,6 +600,9 @@ class _DeviceBlock:
     the last view is gone."""
 
     __slots__ = ("ptr", "stream", "__cuda_array_interface__", "__weakref__")
+    # (held by the class: module globals may already be gone when the last
+    # view dies at interpreter shutdown)
+    _free = _lib.nlb_device_free
 
     def __init__(self, ptr: int, shape, typestr: str, stream: int):
         self.ptr = ptr
@@ -610,7 +613,10 @@ class _DeviceBlock:
 
     def __del__(self):
         if self.ptr:
-            _lib.nlb_device_free(ctypes.c_void_p(self.ptr), ctypes.c_void_p(self.stream))
+            try:
+                self._free(self.ptr, self.stream)
+            except Exception:  # interpreter shutdown
+                pass
             self.ptr = 0
 
 
