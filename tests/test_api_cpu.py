@@ -216,3 +216,30 @@ def test_batch_validation_with_and_without_offsets(nl, offsets):
                                      return_offsets=offsets)
     assert r["edge_index"].shape == (2, 0)
     assert ("system_offsets" in r) == offsets
+
+
+def test_device_block_release_survives_module_teardown(nl, monkeypatch):
+    """A zero-copy device result whose last view dies after the module's
+    globals are gone (interpreter shutdown) still calls the library's free
+    function held by its class, and never raises."""
+    calls = []
+
+    class FakeFree:
+        def __call__(self, ptr, stream):
+            calls.append((ptr, stream))
+            return 0
+
+    monkeypatch.setattr(nl._DeviceBlock, "_free", FakeFree())
+    monkeypatch.setattr(nl, "_lib", None)
+    b = nl._DeviceBlock(0x1000, (2, 3), "<i8", 7)
+    assert b.__cuda_array_interface__["shape"] == (2, 3)
+    del b
+    assert calls == [(0x1000, 7)]
+
+    class Raising:
+        def __call__(self, ptr, stream):
+            raise RuntimeError("no CUDA context")
+
+    monkeypatch.setattr(nl._DeviceBlock, "_free", Raising())
+    b = nl._DeviceBlock(0x2000, (1,), "<i4", 0)
+    del b  # swallowed, as at interpreter shutdown
